@@ -1,0 +1,468 @@
+// C-ABI entry points of libhodlr_b200.so.
+//
+// The hmat_lib functions keep their signatures, argument meaning, ownership
+// rules and error behaviour (include/hmat_lib/*.h); the arithmetic runs on
+// the GPU.  Every failure is reported through *ierr (and the message through
+// hodlr_b200_last_error()); nothing falls back to the CPU.
+#include <cstring>
+#include <memory>
+
+#include "../../include/hmat_lib/constructors.h"
+#include "../../include/hmat_lib/dense_algebra.h"
+#include "../../include/hmat_lib/hodlr_algebra.h"
+#include "../../include/hmat_lib/hodlr_b200.h"
+#include "../../include/hmat_lib/utils.h"
+#include "../../include/hmat_lib/vector_algebra.h"
+#include "build.h"
+#include "hxh.h"
+#include "products.h"
+
+using namespace hb;
+
+struct hodlr_b200_tree_s {
+  std::shared_ptr<DeviceTree> p;
+};
+
+namespace {
+
+int fail(int *ierr, const Error &e) {
+  set_last_error(e.msg);
+  if (ierr) *ierr = e.code;
+  return e.code;
+}
+
+cudaStream_t as_stream(void *s) { return s ? (cudaStream_t)s : lib_stream(); }
+
+// Leaf sizes of a tree of height h over m rows with halving splits, the
+// top-left child taking m - m/2 (hmat_lib src/constructors.c:60-64).
+std::vector<int> halves(int m, int h) {
+  std::vector<int> sizes{m};
+  for (int l = 0; l < h; ++l) {
+    std::vector<int> nxt;
+    for (int s : sizes) {
+      nxt.push_back(s - s / 2);
+      nxt.push_back(s / 2);
+    }
+    sizes.swap(nxt);
+  }
+  return sizes;
+}
+
+// Writes every node size of the host tree from its leaf sizes, as hmat_lib's
+// block sizing does (src/constructors.c:44-176).
+void apply_sizes(TreeHODLR *t, const std::vector<int> &leaf) {
+  const int h = t->height;
+  std::vector<long long> off(leaf.size() + 1, 0);
+  for (size_t i = 0; i < leaf.size(); ++i) off[i + 1] = off[i] + leaf[i];
+  for (int i = 0; i < (1 << h); ++i) diag_leaf(t->root, h, i)->data.diagonal.m = leaf[i];
+  for (int d = 0; d < h; ++d)
+    for (int j = 0; j < (1 << d); ++j) {
+      HODLRInternalNode *node = node_at(t->root, d, j);
+      const int span = 1 << (h - d);
+      const int a = (int)(off[j * span + span / 2] - off[j * span]);
+      const int b = (int)(off[(j + 1) * span] - off[j * span + span / 2]);
+      node->m = a + b;
+      node->children[1].leaf->data.off_diagonal.m = a;
+      node->children[1].leaf->data.off_diagonal.n = b;
+      node->children[2].leaf->data.off_diagonal.m = b;
+      node->children[2].leaf->data.off_diagonal.n = a;
+    }
+}
+
+struct DevBuf {
+  double *p = nullptr;
+  cudaStream_t s;
+  explicit DevBuf(size_t elems, cudaStream_t st) : s(st) { p = dev_alloc(elems, st); }
+  ~DevBuf() { dev_free(p, s); }
+};
+
+// Host matrix (rows x cols, ld) -> packed device buffer (ld = rows).
+void h2d(double *dst, const double *src, long long rows, long long cols, long long ld,
+         cudaStream_t s) {
+  if (rows * cols == 0) return;
+  HB_CUDA(cudaMemcpy2DAsync(dst, rows * sizeof(double), src, ld * sizeof(double),
+                            rows * sizeof(double), cols, cudaMemcpyHostToDevice, s));
+}
+void d2h(double *dst, long long ld, const double *src, long long rows, long long cols,
+         cudaStream_t s) {
+  if (rows * cols == 0) return;
+  HB_CUDA(cudaMemcpy2DAsync(dst, ld * sizeof(double), src, rows * sizeof(double),
+                            rows * sizeof(double), cols, cudaMemcpyDeviceToHost, s));
+}
+
+// Host-buffer product shared by multiply_vector / multiply_*_dense.
+// X is xr x xc (ld ldx); Y has the same shape (ld ldy).
+void host_product(DeviceTree &t, ProdOp op, const double *X, long long xr, long long xc,
+                  long long ldx, double *Y, long long ldy) {
+  cudaStream_t s = lib_stream();
+  DevBuf dx(xr * xc, s), dy(xr * xc, s);
+  h2d(dx.p, X, xr, xc, ldx, s);
+  const int k = (int)(op == ProdOp::L ? xr : xc);
+  product_f64(t, op, dx.p, k, xr, dy.p, xr, s);
+  d2h(Y, ldy, dy.p, xr, xc, s);
+  HB_CUDA(cudaStreamSynchronize(s));
+}
+
+std::shared_ptr<DeviceTree> subtree_device(const HODLRInternalNode *internal, int height,
+                                           cudaStream_t s) {
+  Geometry g = geometry_of_subtree(internal, height);
+  std::shared_ptr<DeviceTree> dt = dtree_create(g, s);
+  dtree_upload(*dt, const_cast<HODLRInternalNode *>(internal), s);
+  return dt;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------ construction
+
+int dense_to_tree_hodlr(TreeHODLR *hodlr, const int m, const int *ms, double *matrix,
+                        const double svd_threshold, int *ierr) {
+  if (hodlr == nullptr || matrix == nullptr) {
+    *ierr = INPUT_ERROR;
+    return 0;
+  }
+  *ierr = SUCCESS;
+  try {
+    const int h = hodlr->height;
+    std::vector<int> leaf;
+    if (ms == nullptr) {
+      leaf = halves(m, h);
+    } else {
+      leaf.assign(ms, ms + (1 << h));
+      long long total = 0;
+      for (int v : leaf) {
+        HB_REQUIRE(v >= 0, INPUT_ERROR, "negative block size");
+        total += v;
+      }
+      apply_sizes(hodlr, leaf);
+      if (total != m) {
+        *ierr = INPUT_ERROR;   // hmat_lib src/constructors.c:652-655
+        set_last_error("block sizes do not add up to m");
+        return 0;
+      }
+    }
+    apply_sizes(hodlr, leaf);
+    Geometry g = geometry_of(hodlr);
+    cudaStream_t s = lib_stream();
+    DevBuf da((size_t)m * m, s);
+    h2d(da.p, matrix, m, m, m, s);
+    int status = SUCCESS;
+    std::shared_ptr<DeviceTree> dt = build_from_dense(g, da.p, m, svd_threshold, s, &status);
+    dtree_download(*dt, hodlr, s);
+    register_device_tree(hodlr, dt);
+    if (status != SUCCESS) {
+      *ierr = status;
+      set_last_error("Jacobi SVD did not converge within the sweep limit");
+      return 1;
+    }
+    return 0;
+  } catch (const Error &e) {
+    fail(ierr, e);
+    return 0;
+  }
+}
+
+// ---------------------------------------------------------------- products
+
+double *multiply_vector(const TreeHODLR *hodlr, const double *vector, double *out, int *ierr) {
+  if (hodlr == nullptr || vector == nullptr || vector == out) {
+    *ierr = INPUT_ERROR;
+    return nullptr;
+  }
+  bool owned = false;
+  try {
+    const int n = hodlr->root ? geometry_of(hodlr).n : 0;
+    if (out == nullptr) {
+      out = (double *)host_malloc((size_t)n * sizeof(double));
+      if (out == nullptr) {
+        *ierr = ALLOCATION_FAILURE;
+        return nullptr;
+      }
+      owned = true;
+    }
+    *ierr = SUCCESS;
+    auto dt = device_tree_for(hodlr, lib_stream());
+    host_product(*dt, ProdOp::N, vector, n, 1, n, out, n);
+    return out;
+  } catch (const Error &e) {
+    fail(ierr, e);
+    if (owned) host_free(out);
+    return nullptr;
+  }
+}
+
+int compute_multiply_hodlr_dense_workspace(const TreeHODLR *hodlr, const int matrix_a) {
+  return get_highest_s(hodlr) * matrix_a;
+}
+
+static double *dense_entry(const TreeHODLR *hodlr, ProdOp op, const double *matrix, int k,
+                           int matrix_ld, double *out, int out_ld, int *ierr) {
+  if (hodlr == nullptr || matrix == nullptr || matrix == out) {
+    *ierr = INPUT_ERROR;
+    return nullptr;
+  }
+  bool owned = false;
+  try {
+    const int n = geometry_of(hodlr).n;
+    const long long cols = (op == ProdOp::L) ? n : k;   // columns of out
+    if (out == nullptr) {
+      out = (double *)host_malloc((size_t)std::max<long long>((long long)out_ld * cols, 1) *
+                                  sizeof(double));
+      if (out == nullptr) {
+        *ierr = ALLOCATION_FAILURE;
+        return nullptr;
+      }
+      owned = true;
+    }
+    *ierr = SUCCESS;
+    auto dt = device_tree_for(hodlr, lib_stream());
+    if (op == ProdOp::L)
+      host_product(*dt, op, matrix, k, n, matrix_ld, out, out_ld);
+    else
+      host_product(*dt, op, matrix, n, k, matrix_ld, out, out_ld);
+    return out;
+  } catch (const Error &e) {
+    fail(ierr, e);
+    if (owned) host_free(out);
+    return nullptr;
+  }
+}
+
+double *multiply_hodlr_dense(const TreeHODLR *hodlr, const double *matrix, const int matrix_n,
+                             const int matrix_ld, double *out, const int out_ld, int *ierr) {
+  return dense_entry(hodlr, ProdOp::N, matrix, matrix_n, matrix_ld, out, out_ld, ierr);
+}
+
+double *multiply_hodlr_transpose_dense(const TreeHODLR *hodlr, const double *matrix,
+                                       const int matrix_n, const int matrix_ld, double *out,
+                                       const int out_ld, int *ierr) {
+  return dense_entry(hodlr, ProdOp::T, matrix, matrix_n, matrix_ld, out, out_ld, ierr);
+}
+
+double *multiply_dense_hodlr(const TreeHODLR *hodlr, const double *matrix, const int matrix_m,
+                             const int matrix_ld, double *out, const int out_ld, int *ierr) {
+  return dense_entry(hodlr, ProdOp::L, matrix, matrix_m, matrix_ld, out, out_ld, ierr);
+}
+
+// Subtree products have no ierr in hmat_lib; failures are reported through
+// hodlr_b200_last_error() and leave `out` unchanged.
+static void internal_entry(const HODLRInternalNode *internal, int height, ProdOp op,
+                           const double *matrix, int k, int matrix_ld, double *out, int out_ld) {
+  if (internal == nullptr || matrix == nullptr || out == nullptr) {
+    set_last_error("NULL argument");
+    return;
+  }
+  try {
+    cudaStream_t s = lib_stream();
+    auto dt = subtree_device(internal, height, s);
+    const int n = dt->g.n;
+    if (op == ProdOp::L)
+      host_product(*dt, op, matrix, k, n, matrix_ld, out, out_ld);
+    else
+      host_product(*dt, op, matrix, n, k, matrix_ld, out, out_ld);
+  } catch (const Error &e) {
+    set_last_error(e.msg);
+  }
+}
+
+void multiply_internal_node_dense(const HODLRInternalNode *internal, const int height,
+                                  const double *matrix, const int matrix_n, const int matrix_ld,
+                                  const HODLRInternalNode **, double *, double *out,
+                                  const int out_ld) {
+  internal_entry(internal, height, ProdOp::N, matrix, matrix_n, matrix_ld, out, out_ld);
+}
+
+void multiply_internal_node_transpose_dense(const HODLRInternalNode *internal, const int height,
+                                            const double *matrix, const int matrix_n,
+                                            const int matrix_ld, const HODLRInternalNode **,
+                                            double *, double *out, const int out_ld) {
+  internal_entry(internal, height, ProdOp::T, matrix, matrix_n, matrix_ld, out, out_ld);
+}
+
+void multiply_dense_internal_node(const HODLRInternalNode *internal, const int height,
+                                  const double *matrix, const int matrix_m, const int matrix_ld,
+                                  const HODLRInternalNode **, double *, double *out,
+                                  const int out_ld) {
+  internal_entry(internal, height, ProdOp::L, matrix, matrix_m, matrix_ld, out, out_ld);
+}
+
+// ------------------------------------------------------------ HODLR x HODLR
+
+int multiply_hodlr_hodlr(const TreeHODLR *hodlr1, const TreeHODLR *hodlr2, TreeHODLR *out,
+                         const double svd_threshold, int *ierr) {
+  if (hodlr1 == nullptr || hodlr2 == nullptr || out == nullptr) {
+    *ierr = INPUT_ERROR;
+    return 0;
+  }
+  *ierr = SUCCESS;
+  try {
+    HB_REQUIRE(hodlr1->height == hodlr2->height && out->height == hodlr1->height, INPUT_ERROR,
+               "trees of different heights");
+    cudaStream_t s = lib_stream();
+    auto a = device_tree_for(hodlr1, s);
+    auto b = device_tree_for(hodlr2, s);
+    int status = SUCCESS;
+    std::shared_ptr<DeviceTree> c = hxh_multiply(*a, *b, svd_threshold, s, &status);
+    dtree_download(*c, out, s);
+    register_device_tree(out, c);
+    if (status != SUCCESS) {
+      *ierr = status;
+      set_last_error("SVD of a recompression did not converge");
+      return 1;
+    }
+    return 0;
+  } catch (const Error &e) {
+    fail(ierr, e);
+    return 0;
+  }
+}
+
+// ------------------------------------------------------------ extensions
+
+const char *hodlr_b200_version(void) { return "hodlr-b200 0.1 (sm_100a)"; }
+const char *hodlr_b200_last_error(void) { return last_error(); }
+long long hodlr_b200_kernel_launches(void) { return launches(); }
+
+int hodlr_b200_set_option(const char *name, double value) {
+  if (!name) return INPUT_ERROR;
+  set_option(name, value);
+  return SUCCESS;
+}
+
+void hodlr_b200_set_host_allocator(void *(*alloc_fn)(size_t), void (*free_fn)(void *)) {
+  HostAllocator &a = host_allocator();
+  if (alloc_fn && free_fn) {
+    a.alloc = alloc_fn;
+    a.release = free_fn;
+  } else {
+    a.alloc = &std::malloc;
+    a.release = &std::free;
+  }
+}
+
+int hodlr_b200_build_dev(int height, int n, const int *ms, const double *d_matrix, int ld,
+                         double svd_threshold, int flags, void *stream, hodlr_b200_tree *out,
+                         int *ierr) {
+  (void)flags;
+  if (!d_matrix || !out || height < 1 || n < 0) {
+    if (ierr) *ierr = INPUT_ERROR;
+    return INPUT_ERROR;
+  }
+  try {
+    Geometry g;
+    g.h = height;
+    std::vector<int> leaf = ms ? std::vector<int>(ms, ms + (1 << height)) : halves(n, height);
+    g.leaf_m = leaf;
+    g.leaf_off.assign(leaf.size() + 1, 0);
+    for (size_t i = 0; i < leaf.size(); ++i) g.leaf_off[i + 1] = g.leaf_off[i] + leaf[i];
+    HB_REQUIRE(g.leaf_off.back() == n, INPUT_ERROR, "block sizes do not add up to n");
+    g.n = n;
+    g.blocks.resize(g.nblock());
+    for (int d = 0; d < height; ++d)
+      for (int j = 0; j < (1 << d); ++j) {
+        const int span = 1 << (height - d);
+        const long long o = g.leaf_off[j * span], mid = g.leaf_off[j * span + span / 2],
+                        end = g.leaf_off[(j + 1) * span];
+        BlockDesc &tr = g.blocks[block_index(d, j, 1)];
+        BlockDesc &bl = g.blocks[block_index(d, j, 2)];
+        tr = BlockDesc{(int)o, (int)mid, (int)(mid - o), (int)(end - mid), 0, d, 0, 0};
+        bl = BlockDesc{(int)mid, (int)o, (int)(end - mid), (int)(mid - o), 0, d, 0, 0};
+      }
+    int status = SUCCESS;
+    auto dt = build_from_dense(g, d_matrix, ld, svd_threshold, as_stream(stream), &status);
+    *out = new hodlr_b200_tree_s{dt};
+    if (ierr) *ierr = status;
+    return status;
+  } catch (const Error &e) {
+    return fail(ierr, e);
+  }
+}
+
+void hodlr_b200_tree_free(hodlr_b200_tree t) { delete t; }
+
+int hodlr_b200_tree_to_host(hodlr_b200_tree t, TreeHODLR *hodlr, int *ierr) {
+  if (!t || !hodlr || hodlr->height != t->p->g.h) {
+    if (ierr) *ierr = INPUT_ERROR;
+    return INPUT_ERROR;
+  }
+  try {
+    dtree_download(*t->p, hodlr, lib_stream());
+    register_device_tree(hodlr, t->p);
+    if (ierr) *ierr = SUCCESS;
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(ierr, e);
+  }
+}
+
+hodlr_b200_tree hodlr_b200_tree_from_host(const TreeHODLR *hodlr, int *ierr) {
+  try {
+    auto dt = device_tree_for(hodlr, lib_stream());
+    if (ierr) *ierr = SUCCESS;
+    return new hodlr_b200_tree_s{dt};
+  } catch (const Error &e) {
+    fail(ierr, e);
+    return nullptr;
+  }
+}
+
+int hodlr_b200_tree_info(hodlr_b200_tree t, int *height, int *n, int *max_rank,
+                         long long *storage_doubles, long long *arena_bytes) {
+  if (!t) return INPUT_ERROR;
+  if (height) *height = t->p->g.h;
+  if (n) *n = t->p->g.n;
+  if (max_rank) *max_rank = t->p->g.max_rank();
+  if (storage_doubles) *storage_doubles = t->p->storage();
+  if (arena_bytes) *arena_bytes = t->p->arena_elems * (long long)sizeof(double);
+  return SUCCESS;
+}
+
+int hodlr_b200_tree_ranks(hodlr_b200_tree t, int *ranks, int capacity) {
+  if (!t) return -1;
+  const int nb = t->p->g.nblock();
+  for (int b = 0; b < nb && b < capacity; ++b) ranks[b] = t->p->g.blocks[b].s;
+  return nb;
+}
+
+int hodlr_b200_matmat_dev(hodlr_b200_tree t, int op, int precision, const double *d_x, int k,
+                          int ldx, double *d_y, int ldy, void *stream) {
+  if (!t || !d_x || !d_y || op < 0 || op > 2) return INPUT_ERROR;
+  try {
+    HB_REQUIRE(precision == HODLR_B200_FP64, INPUT_ERROR, "precision mode not available");
+    product_f64(*t->p, (ProdOp)op, d_x, k, ldx, d_y, ldy, as_stream(stream));
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshold,
+                       hodlr_b200_tree *out, int *ierr) {
+  if (!a || !b || !out) {
+    if (ierr) *ierr = INPUT_ERROR;
+    return INPUT_ERROR;
+  }
+  try {
+    int status = SUCCESS;
+    auto c = hxh_multiply(*a->p, *b->p, svd_threshold, lib_stream(), &status);
+    *out = new hodlr_b200_tree_s{c};
+    if (ierr) *ierr = status;
+    return status;
+  } catch (const Error &e) {
+    return fail(ierr, e);
+  }
+}
+
+int hodlr_b200_sync_tree(const TreeHODLR *hodlr) {
+  try {
+    forget_device_tree(hodlr);
+    device_tree_for(hodlr, lib_stream());
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+}  // extern "C"

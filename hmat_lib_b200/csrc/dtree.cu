@@ -1,0 +1,216 @@
+// Device tree arena, upload / download and the host-tree registry.
+#include <cstring>
+#include <unordered_map>
+
+#include "dtree.h"
+#include "products.h"
+
+namespace hb {
+
+namespace {
+std::mutex g_reg_mutex;
+std::unordered_map<const TreeHODLR *, std::shared_ptr<DeviceTree>> g_registry;
+}  // namespace
+
+DeviceTree::~DeviceTree() {
+  plans.clear();
+  if (arena) cudaFree(arena);
+  if (d_leaves) cudaFree(d_leaves);
+  if (d_blocks) cudaFree(d_blocks);
+}
+
+long long DeviceTree::storage() const {
+  long long w = 0;
+  for (int m : g.leaf_m) w += (long long)m * m;
+  for (auto &b : g.blocks) w += (long long)b.s * (b.m + b.n);
+  return w;
+}
+
+cudaStream_t lib_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  HB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  streams[dev] = s;
+  return s;
+}
+
+double *dev_alloc(size_t elems, cudaStream_t stream) {
+  void *p = nullptr;
+  HB_CUDA(cudaMallocAsync(&p, std::max<size_t>(elems, 1) * sizeof(double), stream));
+  return (double *)p;
+}
+
+void dev_free(void *p, cudaStream_t stream) {
+  if (p) cudaFreeAsync(p, stream);
+}
+
+std::unique_ptr<DeviceTree> dtree_create(const Geometry &g_in, cudaStream_t stream) {
+  auto t = std::make_unique<DeviceTree>();
+  HB_CUDA(cudaGetDevice(&t->device));
+  t->g = g_in;
+  Geometry &g = t->g;
+  long long off = 0;
+  t->leaves.resize(g.nleaf());
+  for (int i = 0; i < g.nleaf(); ++i) {
+    t->leaves[i] = LeafDesc{(int)g.leaf_off[i], g.leaf_m[i], off};
+    off += align_up((long long)g.leaf_m[i] * g.leaf_m[i]);
+  }
+  for (auto &b : g.blocks) {
+    b.u_off = off;
+    off += align_up((long long)b.m * b.s);
+    b.v_off = off;
+    off += align_up((long long)b.n * b.s);
+  }
+  t->arena_elems = off;
+  HB_CUDA(cudaMalloc(&t->arena, std::max<long long>(off, 1) * sizeof(double)));
+  HB_CUDA(cudaMalloc(&t->d_leaves, std::max<size_t>(t->leaves.size(), 1) * sizeof(LeafDesc)));
+  HB_CUDA(cudaMalloc(&t->d_blocks, std::max<size_t>(g.blocks.size(), 1) * sizeof(BlockDesc)));
+  HB_CUDA(cudaMemcpyAsync(t->d_leaves, t->leaves.data(), t->leaves.size() * sizeof(LeafDesc),
+                          cudaMemcpyHostToDevice, stream));
+  if (!g.blocks.empty())
+    HB_CUDA(cudaMemcpyAsync(t->d_blocks, g.blocks.data(), g.blocks.size() * sizeof(BlockDesc),
+                            cudaMemcpyHostToDevice, stream));
+  HB_CUDA(cudaStreamSynchronize(stream));
+  return t;
+}
+
+void dtree_upload(DeviceTree &t, HODLRInternalNode *root, cudaStream_t stream) {
+  const Geometry &g = t.g;
+  // gather into one host staging image of the arena, one copy
+  std::vector<double> img(t.arena_elems, 0.0);
+  for (int i = 0; i < g.nleaf(); ++i) {
+    HODLRLeafNode *leaf = diag_leaf(root, g.h, i);
+    const long long mm = (long long)g.leaf_m[i] * g.leaf_m[i];
+    HB_REQUIRE(mm == 0 || leaf->data.diagonal.data != nullptr, INPUT_ERROR,
+               "diagonal leaf without data");
+    if (mm) std::memcpy(&img[t.leaves[i].off], leaf->data.diagonal.data, mm * sizeof(double));
+  }
+  for (int d = 0; d < g.h; ++d)
+    for (int j = 0; j < (1 << d); ++j) {
+      HODLRInternalNode *node = node_at(root, d, j);
+      for (int c = 1; c <= 2; ++c) {
+        const NodeOffDiagonal &od = node->children[c].leaf->data.off_diagonal;
+        const BlockDesc &b = g.blocks[block_index(d, j, c)];
+        const long long mu = (long long)b.m * b.s, mv = (long long)b.n * b.s;
+        HB_REQUIRE((mu == 0 || od.u != nullptr) && (mv == 0 || od.v != nullptr), INPUT_ERROR,
+                   "off-diagonal leaf without factors");
+        if (mu) std::memcpy(&img[b.u_off], od.u, mu * sizeof(double));
+        if (mv) std::memcpy(&img[b.v_off], od.v, mv * sizeof(double));
+      }
+    }
+  if (t.arena_elems)
+    HB_CUDA(cudaMemcpyAsync(t.arena, img.data(), t.arena_elems * sizeof(double),
+                            cudaMemcpyHostToDevice, stream));
+  HB_CUDA(cudaStreamSynchronize(stream));
+}
+
+void dtree_download(const DeviceTree &t, TreeHODLR *host, cudaStream_t stream) {
+  const Geometry &g = t.g;
+  std::vector<double> img(t.arena_elems);
+  if (t.arena_elems)
+    HB_CUDA(cudaMemcpyAsync(img.data(), t.arena, t.arena_elems * sizeof(double),
+                            cudaMemcpyDeviceToHost, stream));
+  HB_CUDA(cudaStreamSynchronize(stream));
+  auto copy_out = [&](long long off, long long count) -> double * {
+    auto *p = (double *)host_malloc(std::max<long long>(count, 1) * sizeof(double));
+    HB_REQUIRE(p != nullptr, ALLOCATION_FAILURE, "host allocation of tree data failed");
+    if (count) std::memcpy(p, &img[off], count * sizeof(double));
+    return p;
+  };
+  for (int i = 0; i < g.nleaf(); ++i) {
+    HODLRLeafNode *leaf = diag_leaf(host->root, g.h, i);
+    leaf->data.diagonal.m = g.leaf_m[i];
+    leaf->data.diagonal.data = copy_out(t.leaves[i].off, (long long)g.leaf_m[i] * g.leaf_m[i]);
+  }
+  for (int d = 0; d < g.h; ++d)
+    for (int j = 0; j < (1 << d); ++j) {
+      HODLRInternalNode *node = node_at(host->root, d, j);
+      const int span = 1 << (g.h - d);
+      node->m = (int)(g.leaf_off[(j + 1) * span] - g.leaf_off[j * span]);
+      for (int c = 1; c <= 2; ++c) {
+        NodeOffDiagonal &od = node->children[c].leaf->data.off_diagonal;
+        const BlockDesc &b = g.blocks[block_index(d, j, c)];
+        od.m = b.m;
+        od.n = b.n;
+        od.s = b.s;
+        od.u = copy_out(b.u_off, (long long)b.m * b.s);
+        od.v = copy_out(b.v_off, (long long)b.n * b.s);
+      }
+    }
+}
+
+// FNV-1a over the tree's structure, data pointers and a few values of every
+// buffer.  Detects a different tree at a reused address; in-place edits of
+// factor values that leave the sampled entries unchanged must be announced
+// with hodlr_b200_sync_tree().
+uint64_t host_fingerprint(const TreeHODLR *t) {
+  uint64_t h = 1469598103934665603ULL;
+  auto mix = [&](const void *p, size_t n) {
+    auto *c = (const unsigned char *)p;
+    for (size_t i = 0; i < n; ++i) {
+      h ^= c[i];
+      h *= 1099511628211ULL;
+    }
+  };
+  auto sample = [&](const double *x, long long count) {
+    mix(&x, sizeof(x));
+    mix(&count, sizeof(count));
+    if (!x || count <= 0) return;
+    const long long idx[5] = {0, count / 4, count / 2, (3 * count) / 4, count - 1};
+    for (long long i : idx) mix(&x[i], sizeof(double));
+  };
+  mix(&t->height, sizeof(int));
+  const Geometry g = geometry_of(t);
+  for (int i = 0; i < g.nleaf(); ++i) {
+    HODLRLeafNode *leaf = diag_leaf(t->root, g.h, i);
+    sample(leaf->data.diagonal.data, (long long)g.leaf_m[i] * g.leaf_m[i]);
+  }
+  for (int d = 0; d < g.h; ++d)
+    for (int j = 0; j < (1 << d); ++j) {
+      HODLRInternalNode *node = node_at(t->root, d, j);
+      for (int c = 1; c <= 2; ++c) {
+        const NodeOffDiagonal &od = node->children[c].leaf->data.off_diagonal;
+        mix(&od.s, sizeof(int));
+        sample(od.u, (long long)od.m * od.s);
+        sample(od.v, (long long)od.n * od.s);
+      }
+    }
+  return h;
+}
+
+void register_device_tree(const TreeHODLR *t, std::shared_ptr<DeviceTree> dt) {
+  dt->fingerprint = host_fingerprint(t);
+  std::lock_guard<std::mutex> lk(g_reg_mutex);
+  g_registry[t] = std::move(dt);
+}
+
+std::shared_ptr<DeviceTree> device_tree_for(const TreeHODLR *t, cudaStream_t stream) {
+  HB_REQUIRE(t != nullptr && t->root != nullptr, INPUT_ERROR, "NULL tree");
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  const uint64_t fp = host_fingerprint(t);
+  {
+    std::lock_guard<std::mutex> lk(g_reg_mutex);
+    auto it = g_registry.find(t);
+    if (it != g_registry.end() && it->second->fingerprint == fp && it->second->device == dev)
+      return it->second;
+  }
+  Geometry g = geometry_of(t);
+  std::shared_ptr<DeviceTree> dt = dtree_create(g, stream);
+  dtree_upload(*dt, t->root, stream);
+  dt->fingerprint = fp;
+  std::lock_guard<std::mutex> lk(g_reg_mutex);
+  g_registry[t] = dt;
+  return dt;
+}
+
+void forget_device_tree(const TreeHODLR *t) {
+  std::lock_guard<std::mutex> lk(g_reg_mutex);
+  g_registry.erase(t);
+}
+
+}  // namespace hb

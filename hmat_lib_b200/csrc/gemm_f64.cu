@@ -1,0 +1,336 @@
+// FP64 variable-batched segmented GEMM for sm_100a.
+//
+// CUDA-core DFMA kernel: 256 threads, a BM x BN output tile per CTA
+// (128 x 64 or 64 x 128), K advanced 16 at a time through a two-stage
+// cp.async pipeline (8-byte copies with zero fill, so any leading dimension
+// and any offset work), 32 accumulators per thread, operands read from shared
+// memory as double2.  FP64 has no tcgen05 path; this is the FP64 roofline
+// kernel (B200: 64 DFMA / clock / SM).
+#include <algorithm>
+#include <cstring>
+
+#include "gemm_f64.h"
+
+namespace hb {
+
+namespace {
+
+constexpr int kBK = 16;
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+struct KIter {
+  int si;      // segment index (absolute)
+  int kk;      // position inside the segment
+  int le;      // end of the valid range inside the segment
+  int kbase;   // concatenated-K position of the segment start
+};
+
+template <int BM, int BN>
+struct Smem {
+  static constexpr int LDA = BM + 2;
+  static constexpr int LDB = BN + 2;
+  static constexpr size_t bytes = sizeof(double) * 2 * kBK * (LDA + LDB);
+};
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(kThreads, 2)
+gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ probs,
+                const GemmTile *__restrict__ tiles, GemmBases bases) {
+  constexpr int TM = BM / 16, TN = BN / 16;
+  constexpr int LDA = Smem<BM, BN>::LDA, LDB = Smem<BM, BN>::LDB;
+  extern __shared__ __align__(16) double smem[];
+  double *As = smem;                        // [2][kBK][LDA]
+  double *Bs = smem + 2 * kBK * LDA;        // [2][kBK][LDB]
+
+  const GemmTile tile = tiles[blockIdx.x];
+  const GemmProb P = probs[tile.prob];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int seg_end = P.seg0 + P.nseg;
+
+  double acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0;
+
+  auto settle = [&](KIter &it) {
+    while (it.si < seg_end) {
+      const int K = segs[it.si].K;
+      const int ls = max(tile.k0 - it.kbase, 0);
+      const int le = min(tile.k1 - it.kbase, K);
+      if (ls < le) {
+        it.kk = ls;
+        it.le = le;
+        return;
+      }
+      it.kbase += K;
+      ++it.si;
+    }
+  };
+  auto advance = [&](KIter &it) {
+    it.kk += kBK;
+    if (it.kk >= it.le) {
+      it.kbase += segs[it.si].K;
+      ++it.si;
+      settle(it);
+    }
+  };
+
+  auto load = [&](int buf, const KIter &it) {
+    const GemmSeg S = segs[it.si];
+    const double *A = bases.p[S.abase] + S.a_off;
+    const double *B = bases.p[S.bbase] + S.b_off;
+    double *as = As + buf * kBK * LDA;
+    double *bs = Bs + buf * kBK * LDB;
+    const int kk = it.kk, kend = it.le;
+    if (S.ta == 0) {
+      constexpr int KS = kThreads / BM;
+      const int m = tid % BM;
+      const bool mok = (tile.m0 + m) < P.M;
+#pragma unroll
+      for (int i = 0; i < BM * kBK / kThreads; ++i) {
+        const int k = tid / BM + KS * i;
+        const bool p = mok && (kk + k) < kend;
+        const double *src = p ? A + (tile.m0 + m) + (long long)(kk + k) * S.lda : A;
+        cp_async8(as + k * LDA + m, src, p);
+      }
+    } else {
+      const int k = tid & 15;
+      const bool kok = (kk + k) < kend;
+#pragma unroll
+      for (int i = 0; i < BM / 16; ++i) {
+        const int m = (tid >> 4) + 16 * i;
+        const bool p = kok && (tile.m0 + m) < P.M;
+        const double *src = p ? A + (kk + k) + (long long)(tile.m0 + m) * S.lda : A;
+        cp_async8(as + k * LDA + m, src, p);
+      }
+    }
+    if (S.tb == 0) {
+      const int k = tid & 15;
+      const bool kok = (kk + k) < kend;
+#pragma unroll
+      for (int i = 0; i < BN / 16; ++i) {
+        const int n = (tid >> 4) + 16 * i;
+        const bool p = kok && (tile.n0 + n) < P.N;
+        const double *src = p ? B + (kk + k) + (long long)(tile.n0 + n) * S.ldb : B;
+        cp_async8(bs + k * LDB + n, src, p);
+      }
+    } else {
+      constexpr int KS = kThreads / BN;
+      const int n = tid % BN;
+      const bool nok = (tile.n0 + n) < P.N;
+#pragma unroll
+      for (int i = 0; i < BN * kBK / kThreads; ++i) {
+        const int k = tid / BN + KS * i;
+        const bool p = nok && (kk + k) < kend;
+        const double *src = p ? B + (tile.n0 + n) + (long long)(kk + k) * S.ldb : B;
+        cp_async8(bs + k * LDB + n, src, p);
+      }
+    }
+  };
+
+  KIter it{P.seg0, 0, 0, 0};
+  settle(it);
+  int buf = 0;
+  if (it.si < seg_end) load(0, it);
+  cp_async_commit();
+  while (it.si < seg_end) {
+    KIter nx = it;
+    advance(nx);
+    if (nx.si < seg_end) load(buf ^ 1, nx);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const double *as = As + buf * kBK * LDA;
+    const double *bs = Bs + buf * kBK * LDB;
+#pragma unroll
+    for (int k = 0; k < kBK; ++k) {
+      double a[TM], b[TN];
+#pragma unroll
+      for (int i = 0; i < TM / 2; ++i) {
+        const double2 v = *reinterpret_cast<const double2 *>(as + k * LDA + 2 * ty + 32 * i);
+        a[2 * i] = v.x;
+        a[2 * i + 1] = v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < TN / 2; ++j) {
+        const double2 v = *reinterpret_cast<const double2 *>(bs + k * LDB + 2 * tx + 32 * j);
+        b[2 * j] = v.x;
+        b[2 * j + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+    buf ^= 1;
+    it = nx;
+  }
+  cp_async_wait<0>();
+
+  double *C = bases.p[P.cbase] + P.c_off;
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const int m = tile.m0 + 2 * ty + 32 * (i >> 1) + (i & 1);
+    if (m >= P.M) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int n = tile.n0 + 2 * tx + 32 * (j >> 1) + (j & 1);
+      if (n >= P.N) continue;
+      double *c = C + m + (long long)n * P.ldc;
+      const double v = P.alpha * acc[i][j];
+      if (P.split > 1)
+        atomicAdd(c, v);
+      else
+        *c = (P.beta == 0.0) ? v : v + P.beta * (*c);
+    }
+  }
+}
+
+// beta pre-pass for problems whose tiles accumulate with atomics
+__global__ void gemm_scale_c_kernel(const GemmProb *__restrict__ probs, int nprobs,
+                                    GemmBases bases) {
+  for (int p = blockIdx.y; p < nprobs; p += gridDim.y) {
+    const GemmProb P = probs[p];
+    if (P.split <= 1) continue;
+    double *C = bases.p[P.cbase] + P.c_off;
+    const long long total = (long long)P.M * P.N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+      const long long m = e % P.M, n = e / P.M;
+      double *c = C + m + n * P.ldc;
+      *c = (P.beta == 0.0) ? 0.0 : P.beta * (*c);
+    }
+  }
+}
+
+template <int BM, int BN>
+void launch_gemm(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stream) {
+  static bool configured = false;
+  const size_t smem = Smem<BM, BN>::bytes;
+  if (!configured) {
+    HB_CUDA(cudaFuncSetAttribute(gemm_f64_kernel<BM, BN>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  gemm_f64_kernel<BM, BN><<<plan.ntiles, kThreads, smem, stream>>>(plan.segs, plan.probs,
+                                                                   plan.tiles, bases);
+  HB_LAUNCHED();
+}
+
+}  // namespace
+
+GemmPlan::~GemmPlan() {
+  if (dev) cudaFree(dev);
+}
+
+void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool allow_split,
+                     cudaStream_t stream) {
+  const int BM = shape == TileShape::M128N64 ? 128 : 64;
+  const int BN = shape == TileShape::M128N64 ? 64 : 128;
+  plan.shape = shape;
+  auto &probs = batch.probs;
+  std::vector<long long> ktot(probs.size(), 0);
+  long long base_tiles = 0;
+  double work = 0.0;
+  for (size_t p = 0; p < probs.size(); ++p) {
+    for (int s = 0; s < probs[p].nseg; ++s) ktot[p] += batch.segs[probs[p].seg0 + s].K;
+    const long long mn =
+        (long long)((probs[p].M + BM - 1) / BM) * ((probs[p].N + BN - 1) / BN);
+    base_tiles += mn;
+    work += (double)mn * (double)std::max<long long>(ktot[p], 1);
+  }
+  const long long target = 4LL * num_sms();
+  std::vector<GemmTile> tiles;
+  tiles.reserve(base_tiles);
+  plan.any_split = false;
+  for (size_t p = 0; p < probs.size(); ++p) {
+    GemmProb &P = probs[p];
+    if (P.M <= 0 || P.N <= 0) continue;
+    const int mt = (P.M + BM - 1) / BM, nt = (P.N + BN - 1) / BN;
+    long long split = 1;
+    if (allow_split && base_tiles < target && ktot[p] > 4 * 256) {
+      const double share = (double)mt * nt * (double)ktot[p] / work;
+      split = (long long)(share * (double)target / (double)(mt * nt) + 0.5);
+      split = std::max<long long>(1, std::min<long long>(split, ktot[p] / 256));
+    }
+    long long chunk = (ktot[p] + split - 1) / split;
+    chunk = (chunk + kBK - 1) / kBK * kBK;
+    if (chunk <= 0) chunk = kBK;
+    split = std::max<long long>(1, (ktot[p] + chunk - 1) / chunk);
+    P.split = (int)split;
+    if (split > 1) plan.any_split = true;
+    for (int mi = 0; mi < mt; ++mi)
+      for (int ni = 0; ni < nt; ++ni)
+        for (long long si = 0; si < split; ++si) {
+          GemmTile t;
+          t.prob = (int)p;
+          t.m0 = mi * BM;
+          t.n0 = ni * BN;
+          t.k0 = (int)(si * chunk);
+          t.k1 = (int)std::min<long long>(ktot[p], (si + 1) * chunk);
+          if (split == 1) t.k1 = (int)ktot[p];
+          tiles.push_back(t);
+        }
+  }
+  // longest K ranges first for load balance
+  std::stable_sort(tiles.begin(), tiles.end(), [](const GemmTile &a, const GemmTile &b) {
+    return (a.k1 - a.k0) > (b.k1 - b.k0);
+  });
+  plan.ntiles = (int)tiles.size();
+  plan.nprobs = (int)probs.size();
+  const size_t bs = batch.segs.size() * sizeof(GemmSeg);
+  const size_t bp = probs.size() * sizeof(GemmProb);
+  const size_t bt = tiles.size() * sizeof(GemmTile);
+  const size_t total = align_up(bs, 256) + align_up(bp, 256) + align_up(bt, 256) + 256;
+  if (plan.dev) {
+    cudaFree(plan.dev);
+    plan.dev = nullptr;
+  }
+  HB_CUDA(cudaMalloc(&plan.dev, total));
+  char *base = (char *)plan.dev;
+  plan.segs = (GemmSeg *)base;
+  plan.probs = (GemmProb *)(base + align_up(bs, 256));
+  plan.tiles = (GemmTile *)(base + align_up(bs, 256) + align_up(bp, 256));
+  std::vector<char> host(total, 0);
+  if (bs) std::memcpy(host.data(), batch.segs.data(), bs);
+  if (bp) std::memcpy(host.data() + align_up(bs, 256), probs.data(), bp);
+  if (bt) std::memcpy(host.data() + align_up(bs, 256) + align_up(bp, 256), tiles.data(), bt);
+  // pageable source: staged by the driver before the call returns
+  HB_CUDA(cudaMemcpyAsync(plan.dev, host.data(), total, cudaMemcpyHostToDevice, stream));
+  HB_CUDA(cudaStreamSynchronize(stream));
+}
+
+void gemm_plan_run(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stream) {
+  if (plan.ntiles == 0) return;
+  if (plan.any_split) {
+    dim3 grid(64, std::min(plan.nprobs, 1024));
+    gemm_scale_c_kernel<<<grid, 256, 0, stream>>>(plan.probs, plan.nprobs, bases);
+    HB_LAUNCHED();
+  }
+  if (plan.shape == TileShape::M128N64)
+    launch_gemm<128, 64>(plan, bases, stream);
+  else
+    launch_gemm<64, 128>(plan, bases, stream);
+}
+
+void gemm_f64_run(GemmBatch &batch, const GemmBases &bases, TileShape shape, cudaStream_t stream,
+                  bool allow_split) {
+  if (batch.empty()) return;
+  GemmPlan plan;
+  gemm_plan_build(plan, batch, shape, allow_split, stream);
+  gemm_plan_run(plan, bases, stream);
+  HB_CUDA(cudaStreamSynchronize(stream));
+}
+
+}  // namespace hb

@@ -1,0 +1,63 @@
+// Batched FP64 one-sided Jacobi SVD and batched 2-D copies.
+#pragma once
+
+#include "common.h"
+
+namespace hb {
+
+// One SVD problem.  The input block A (m x n, column-major, ld lda) is read
+// only.  With R = max(m, n) and C = min(m, n) the kernel orthogonalises the C
+// columns of the tall orientation in G (R x C, ld R) while accumulating the
+// rotations in W (C x C, ld C).
+struct JacobiProb {
+  const double *A;
+  long long lda;
+  int m, n;
+  double *G;        // workspace R x C
+  double *W;        // workspace C x C
+  double *U;        // out: m x C, ld ldu (left vectors, times sigma if scale_u)
+  long long ldu;
+  double *V;        // out: n x C, ld ldv (right vectors)
+  long long ldv;
+  double *sigma;    // out: C singular values, descending
+  int *rank;        // out: truncation rank (>= 1 unless the block is empty)
+};
+
+enum class Truncation : int {
+  Relative = 0,   // keep while s[k] >= tol * s[0]; one if s[0] <= tol
+                  // (hmat_lib src/constructors.c:329-336)
+  Absolute = 1,   // stop at the first k >= 1 with s[k] <= tol
+                  // (hmat_lib src/hodlr_algebra.c:160-163, 305-308)
+  None = 2,       // keep all C values
+};
+
+struct JacobiParams {
+  double tol = 0.0;
+  Truncation trunc = Truncation::Relative;
+  int scale_u = 1;          // write U * Sigma (hmat_lib stores scaled U)
+  int max_sweeps = 60;      // bounded: exceeding it sets the status word
+  double conv_tol = 1e-15;  // |g_p . g_q| <= conv_tol ||g_p|| ||g_q||
+};
+
+// Workspace doubles needed by problem (m, n): G + W.
+inline long long jacobi_workspace(int m, int n) {
+  const long long R = m > n ? m : n, C = m < n ? m : n;
+  return align_up(R * C) + align_up(C * C);
+}
+
+// status: device int, set to SVD_FAILURE by any problem that did not
+// converge within max_sweeps (left untouched otherwise).
+void jacobi_svd_batched(const JacobiProb *d_probs, int nprobs, const JacobiParams &prm,
+                        int *d_status, int max_c, cudaStream_t stream);
+
+struct CopyDesc {
+  const double *src;
+  long long lds;
+  double *dst;
+  long long ldd;
+  int rows, cols;
+};
+
+void copy2d_batched(const CopyDesc *d_descs, int n, cudaStream_t stream);
+
+}  // namespace hb

@@ -1,0 +1,133 @@
+// HODLR x dense products (FP64) built on the segmented GEMM engine.
+//
+// Replaces hmat_lib src/dense_algebra.c (multiply_hodlr_dense :361,
+// multiply_hodlr_transpose_dense :617, multiply_dense_hodlr :957 and the
+// subtree variants :492, :710, :1087) and src/vector_algebra.c:131
+// (multiply_vector, the k = 1 case).  The reference walks the tree block by
+// block with two dgemm calls per block; here all blocks of all levels run in
+// two launches.
+#include "products.h"
+
+namespace hb {
+
+namespace {
+enum Base { kArena = 0, kX = 1, kY = 2, kW = 3 };
+}
+
+ProductPlan::~ProductPlan() {
+  if (w) cudaFree(w);
+}
+
+ProductWork product_work(const DeviceTree &t, int k) {
+  ProductWork w{};
+  w.elements = (double)t.storage();
+  w.flops = 2.0 * k * w.elements;
+  w.bytes = 8.0 * w.elements + 16.0 * (double)t.g.n * k;
+  return w;
+}
+
+// block (of the node containing leaf i at depth d) whose rows (row_side) or
+// columns (!row_side) cover leaf i
+static int covering_block(int h, int i, int d, bool row_side) {
+  const int j = i >> (h - d);
+  const bool top = ((i >> (h - d - 1)) & 1) == 0;
+  int c;
+  if (row_side)
+    c = top ? 1 : 2;
+  else
+    c = top ? 2 : 1;
+  return block_index(d, j, c);
+}
+
+ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,
+                          cudaStream_t stream) {
+  std::lock_guard<std::mutex> lk(t.plan_mutex);
+  auto key = std::make_tuple((int)op, k, ldx, ldy, (int)Precision::FP64);
+  auto it = t.plans.find(key);
+  if (it != t.plans.end()) return *it->second;
+
+  auto plan = std::make_unique<ProductPlan>();
+  plan->op = op;
+  plan->k = k;
+  plan->ldx = ldx;
+  plan->ldy = ldy;
+  const Geometry &g = t.g;
+  const int h = g.h;
+  std::vector<long long> w_off(g.blocks.size(), 0);
+  long long w_total = 0;
+  for (size_t b = 0; b < g.blocks.size(); ++b) {
+    w_off[b] = w_total;
+    w_total += align_up((long long)g.blocks[b].s * k);
+  }
+  plan->w_elems = w_total;
+  HB_CUDA(cudaMalloc(&plan->w, std::max<long long>(w_total, 1) * sizeof(double)));
+
+  // phase 1: projections
+  GemmBatch p1;
+  for (size_t bi = 0; bi < g.blocks.size(); ++bi) {
+    const BlockDesc &b = g.blocks[bi];
+    if (b.s == 0) continue;
+    if (op == ProdOp::N) {          // W_b (s x k) = V_b^T X[c0 : c0 + n]
+      int p = p1.add(kW, w_off[bi], b.s, b.s, k);
+      p1.seg(p, kArena, b.v_off, b.n, 1, kX, b.c0, ldx, 0, b.n);
+    } else if (op == ProdOp::T) {   // W_b (s x k) = U_b^T X[r0 : r0 + m]
+      int p = p1.add(kW, w_off[bi], b.s, b.s, k);
+      p1.seg(p, kArena, b.u_off, b.m, 1, kX, b.r0, ldx, 0, b.m);
+    } else {                        // Z_b (k x s) = X[:, r0 : r0 + m] U_b
+      int p = p1.add(kW, w_off[bi], k, k, b.s);
+      p1.seg(p, kX, (long long)b.r0 * ldx, ldx, 0, kArena, b.u_off, b.m, 0, b.m);
+    }
+  }
+  // phase 2: one problem per leaf row band (columns for op L)
+  GemmBatch p2;
+  for (int i = 0; i < g.nleaf(); ++i) {
+    const LeafDesc &L = t.leaves[i];
+    if (L.m == 0) continue;
+    if (op == ProdOp::N || op == ProdOp::T) {
+      int p = p2.add(kY, L.r0, ldy, L.m, k);
+      p2.seg(p, kArena, L.off, L.m, op == ProdOp::T ? 1 : 0, kX, L.r0, ldx, 0, L.m);
+      for (int d = h - 1; d >= 0; --d) {
+        const int bi = covering_block(h, i, d, op == ProdOp::N);
+        const BlockDesc &b = g.blocks[bi];
+        if (b.s == 0) continue;
+        if (op == ProdOp::N)
+          p2.seg(p, kArena, b.u_off + (L.r0 - b.r0), b.m, 0, kW, w_off[bi], b.s, 0, b.s);
+        else
+          p2.seg(p, kArena, b.v_off + (L.r0 - b.c0), b.n, 0, kW, w_off[bi], b.s, 0, b.s);
+      }
+    } else {
+      int p = p2.add(kY, (long long)L.r0 * ldy, ldy, k, L.m);
+      p2.seg(p, kX, (long long)L.r0 * ldx, ldx, 0, kArena, L.off, L.m, 0, L.m);
+      for (int d = h - 1; d >= 0; --d) {
+        const int bi = covering_block(h, i, d, false);
+        const BlockDesc &b = g.blocks[bi];
+        if (b.s == 0) continue;
+        p2.seg(p, kW, w_off[bi], k, 0, kArena, b.v_off + (L.r0 - b.c0), b.n, 1, b.s);
+      }
+    }
+  }
+  const TileShape s1 = (op == ProdOp::L) ? TileShape::M128N64 : TileShape::M64N128;
+  const TileShape s2 = (op == ProdOp::L && k <= 64) ? TileShape::M64N128 : TileShape::M128N64;
+  if (!p1.empty()) gemm_plan_build(plan->phase1, p1, s1, true, stream);
+  if (!p2.empty()) gemm_plan_build(plan->phase2, p2, s2, false, stream);
+  auto &ref = *plan;
+  t.plans[key] = std::move(plan);
+  return ref;
+}
+
+void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
+                 long long ldy, cudaStream_t stream) {
+  if (k <= 0 || t.g.n == 0) return;
+  ProductPlan &plan = product_plan(t, op, k, ldx, ldy, stream);
+  GemmBases bases{};
+  bases.p[kArena] = t.arena;
+  bases.p[kX] = const_cast<double *>(X);
+  bases.p[kY] = Y;
+  bases.p[kW] = plan.w;
+  bases.p[4] = t.arena;
+  bases.p[5] = t.arena;
+  gemm_plan_run(plan.phase1, bases, stream);
+  gemm_plan_run(plan.phase2, bases, stream);
+}
+
+}  // namespace hb

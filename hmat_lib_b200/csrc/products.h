@@ -1,0 +1,52 @@
+// HODLR x dense products on the device (FP64).
+#pragma once
+
+#include "dtree.h"
+
+namespace hb {
+
+enum class ProdOp : int {
+  N = 0,  // Y = H X        (hmat_lib src/dense_algebra.c:361)
+  T = 1,  // Y = H^T X      (hmat_lib src/dense_algebra.c:617)
+  L = 2,  // Y = X H        (hmat_lib src/dense_algebra.c:957), X is k x n
+};
+
+enum class Precision : int {
+  FP64 = 0,     // DFMA throughout
+  MIXED = 1,    // split-precision tensor-core products (products_mixed.cu)
+};
+
+// Two launches per product: phase 1 projects the input onto every block's
+// factor (W_b = V_b^T X_b, split along the long dimension with atomics);
+// phase 2 writes each output row band once, accumulating the leaf product and
+// one U_b W_b term per level in registers.
+struct ProductPlan {
+  ProdOp op = ProdOp::N;
+  int k = 0;
+  long long ldx = 0, ldy = 0;
+  GemmPlan phase1, phase2;
+  double *w = nullptr;            // sum_b s_b k doubles of projected input
+  long long w_elems = 0;
+  ProductPlan() = default;
+  ProductPlan(const ProductPlan &) = delete;
+  ProductPlan &operator=(const ProductPlan &) = delete;
+  ~ProductPlan();
+};
+
+// Algorithmic traffic / work of one product (for roofline reporting).
+struct ProductWork {
+  double elements;   // sum m_leaf^2 + sum s (m + n)
+  double flops;      // 2 k elements
+  double bytes;      // 8 elements + 16 n k
+};
+ProductWork product_work(const DeviceTree &t, int k);
+
+// Runs Y = op(H, X) with X, Y device pointers (column-major, ld given).
+void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
+                 long long ldy, cudaStream_t stream);
+
+// Builds (and caches on the tree) the plan for this shape without running it.
+ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,
+                          cudaStream_t stream);
+
+}  // namespace hb

@@ -1,0 +1,78 @@
+/*
+ * Additive API of libhodlr_b200.so (no counterpart in hmat_lib).
+ *
+ * The hmat_lib entry points (allocators.h, constructors.h, vector_algebra.h,
+ * dense_algebra.h, hodlr_algebra.h, utils.h) take host buffers: each call
+ * copies its dense inputs to the GPU and its result back.  A tree built by
+ * dense_to_tree_hodlr() or multiply_hodlr_hodlr() keeps a device copy that
+ * later products reuse; a tree assembled by the caller is uploaded on its
+ * first product and reused while its structure, data pointers and sampled
+ * values are unchanged (call hodlr_b200_sync_tree() after editing factor
+ * values in place).
+ *
+ * The functions below work on device-resident trees and device buffers
+ * directly.  `stream` is a cudaStream_t (NULL: the library's own stream);
+ * they return an ErrorCode (error.h) and never fall back to the CPU.
+ */
+#pragma once
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct TreeHODLR;
+typedef struct hodlr_b200_tree_s *hodlr_b200_tree;
+
+enum HodlrB200Op {
+  HODLR_B200_OP_N = 0,   /* Y = H X   */
+  HODLR_B200_OP_T = 1,   /* Y = H^T X */
+  HODLR_B200_OP_L = 2    /* Y = X H   (X is k x n) */
+};
+
+enum HodlrB200Precision {
+  HODLR_B200_FP64 = 0,   /* FP64 DFMA products */
+  HODLR_B200_MIXED = 1   /* split-precision tensor-core products with FP64 result */
+};
+
+const char *hodlr_b200_version(void);
+/* Message describing the last failure on the calling thread. */
+const char *hodlr_b200_last_error(void);
+/* Runtime knobs, e.g. "jacobi_max_sweeps". Returns SUCCESS. */
+int hodlr_b200_set_option(const char *name, double value);
+/* Allocator for every host buffer the library allocates (tree nodes, factor
+ * copies, results returned for out == NULL).  Both NULL restores malloc/free. */
+void hodlr_b200_set_host_allocator(void *(*alloc_fn)(size_t), void (*free_fn)(void *));
+/* Number of kernels launched by this library so far in this process. */
+long long hodlr_b200_kernel_launches(void);
+
+/* Build from a device-resident n x n column-major matrix (leading dimension
+ * ld), block sizes halved as dense_to_tree_hodlr does (ms == NULL) or given
+ * per leaf (2^height entries).  flags: 0. */
+int hodlr_b200_build_dev(int height, int n, const int *ms, const double *d_matrix, int ld,
+                         double svd_threshold, int flags, void *stream, hodlr_b200_tree *out,
+                         int *ierr);
+void hodlr_b200_tree_free(hodlr_b200_tree t);
+/* Fills an allocated, empty host tree of the same height with copies of the
+ * device factors (library allocator; free with free_tree_data). */
+int hodlr_b200_tree_to_host(hodlr_b200_tree t, struct TreeHODLR *hodlr, int *ierr);
+/* Device handle of a host tree (uploading it if needed); release with
+ * hodlr_b200_tree_free. */
+hodlr_b200_tree hodlr_b200_tree_from_host(const struct TreeHODLR *hodlr, int *ierr);
+int hodlr_b200_tree_info(hodlr_b200_tree t, int *height, int *n, int *max_rank,
+                         long long *storage_doubles, long long *arena_bytes);
+/* Ranks in block order b = 2 * (2^d - 1 + j) + (c - 1); returns the count. */
+int hodlr_b200_tree_ranks(hodlr_b200_tree t, int *ranks, int capacity);
+/* Y = op(H, X) on device buffers (column-major). */
+int hodlr_b200_matmat_dev(hodlr_b200_tree t, int op, int precision, const double *d_x, int k,
+                          int ldx, double *d_y, int ldy, void *stream);
+/* H1 * H2 with recompression at svd_threshold, result stays on the device. */
+int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshold,
+                       hodlr_b200_tree *out, int *ierr);
+/* Re-upload a host tree whose factor values were edited in place. */
+int hodlr_b200_sync_tree(const struct TreeHODLR *hodlr);
+
+#ifdef __cplusplus
+}
+#endif
