@@ -1,0 +1,364 @@
+"""Benchmark: HODLR build + HODLR x dense throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the single-GPU benchmark configuration): n = 32768 points in
+[0,1]^2 (seed 1) in Morton order, Matern-3/2 kernel with length 0.1 plus
+1e-2 I, HODLR depth 8 (leaf 128), truncation tolerance 1e-8; the built
+HODLR times X with 256 columns of N(0,1).  Synthetic data, generated on the
+device.  A step is one H X product; the tree (776 MB of factors) and X
+(64 MB) exceed the 126 MB L2, so no flush is needed between steps.
+
+value  = matmat throughput in algorithmic bytes, B = 8 W + 16 n k per step
+         (W = stored elements), inputs resident in HBM.
+e2e    = the same metric through multiply_hodlr_dense with host buffers
+         (H2D of X and D2H of Y inside every step).
+Printed as one JSON line by rank 0.  With --gpus N > 1 every rank runs an
+independent replica (the product does not shard); value sums the replicas'
+work over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "HODLR build s + matmat GB/s, mixed vs FP64 plain at 1e-8 rel err, 1 B200"
+WORKLOAD = "matern2d_n32768"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=None, help="override n (testing only)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-n", type=int, default=4096)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """cuBLAS DGEMM 8192^3 throughput on this GPU (FP64 roofline denominator;
+    the driver's peak file carries no FP64 figure)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(5):
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def run_cpu_baseline(n: int, k: int):
+    cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--n", str(n),
+           "--height", str(max(1, (n // 128).bit_length() - 1)), "--k", str(k), "--steps", "3"]
+    try:
+        out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+        line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
+        return json.loads(line)
+    except Exception as e:  # the baseline is reported, never required
+        return {"error": str(e)[:200]}
+
+
+def reference_arm(args, rank):
+    """The reference's own CPU implementation (unmodified hmat_lib built in
+    oracle/_ref) on this box's host cores, same metric and unit."""
+    if rank != 0:
+        return
+    res = run_cpu_baseline(args.cpu_n, 256)
+    if "error" in res:
+        print(json.dumps({"impl": "reference", "unavailable": res["error"]}))
+        return
+    nthreads = res["threads"]
+    sample = (f"hmat_lib multiply_hodlr_dense, k=256, on its own build of the same kernel "
+              f"family at n={res['n']} (depth {res['height']}); the reference constructor "
+              f"overflows int at n=32768 (src/constructors.c:676)")
+    value = res["matmat_gbs"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": 3, "warmup": 1, "ms_per_step": res["matmat_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "n": res["n"],
+                                        "height": res["height"], "k": 256, "tol": 1e-8},
+        "build_s": res["build_s"],
+        "build_s_extrapolated_n32768": res["build_s"] * (32768 / res["n"]) ** 3,
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": nthreads,
+                         "kind": "reference", "sample": sample, "cpu": res.get("cpu")},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    from hmat_lib_b200 import abi
+    from hmat_lib_b200 import workloads as W
+    from hmat_lib_b200.hodlr import DeviceTree, Tree, lib as hlib
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=dev)
+        pg = dist
+    lib = hlib()
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+
+    w = W.WORKLOADS[WORKLOAD]
+    n = args.n or w["n"]
+    k, h, tol = w["k"], w["height"] if args.n is None else max(1, (n // 128).bit_length() - 1), w["tol"]
+
+    # ---- input: kernel matrix generated on the device ---------------------------
+    pts = W.workload_points(WORKLOAD, n)
+    d_pts = torch.from_numpy(np.asfortranarray(pts).T.copy().reshape(-1)).to(dev)
+    kind = {"gaussian": 0, "matern32": 1, "exponential": 2}[w["kind"]]
+
+    def make_matrix():
+        a = torch.empty(n * n, dtype=torch.float64, device=dev)
+        r = lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, pts.shape[1], kind,
+                                             w["length"], w["diag"], C.c_void_p(a.data_ptr()), n,
+                                             C.c_void_p(sh))
+        assert r == 0
+        return a
+
+    # ---- build (FP64 plain) -------------------------------------------------------
+    with torch.cuda.stream(stream):
+        a = make_matrix()
+        # warm-up build on a small leading block initialises the kernels
+        DeviceTree.build(a.data_ptr(), 1024, n, 3, tol, stream=sh).free()
+        stream.synchronize()
+        t0 = time.perf_counter()
+        tree = DeviceTree.build(a.data_ptr(), n, n, h, tol, stream=sh)
+        stream.synchronize()
+        build_s = time.perf_counter() - t0
+    info = tree.info()
+    ranks = tree.ranks()
+
+    # ---- accuracy against the dense FP64 product (checker: cuBLAS on A) ------------
+    x = torch.randn(k, n, dtype=torch.float64, device=dev)      # column-major n x k
+    y = torch.zeros(k, n, dtype=torch.float64, device=dev)
+    tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
+    stream.synchronize()
+    a_mat = a.view(n, n)          # row-major view of column-major A = A^T
+    y_dense = (x @ a_mat)         # (k x n) = (A X)^T in column-major terms
+    rel_err = (torch.linalg.norm(y - y_dense) / torch.linalg.norm(y_dense)).item()
+    del a, a_mat, y_dense
+    torch.cuda.empty_cache()
+
+    # ---- timed device-resident products -------------------------------------------
+    storage = info["storage"]
+    bytes_step = 8.0 * storage + 16.0 * n * k
+    flops_step = 2.0 * k * storage
+    for _ in range(args.warmup):
+        tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
+    stream.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    lib.hodlr_b200_set_option(b"record_phase_times", 1.0)
+    lib.hodlr_b200_phase_times(None, 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.hodlr_b200_kernel_launches()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
+        e1.record(stream)
+        stream.synchronize()
+    launches = lib.hodlr_b200_kernel_launches() - launches0
+    lib.hodlr_b200_set_option(b"record_phase_times", 0.0)
+    pt = (C.c_double * 3)()
+    lib.hodlr_b200_phase_times(pt, 3)
+    ms_total = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([ms_total], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_total = t.item()
+        pg.barrier()
+    torch.cuda.synchronize()
+    ms_step = ms_total / args.steps
+    value = bytes_step * world / (ms_step * 1e-3) / 1e9
+
+    # ---- e2e through the C-ABI with host buffers ------------------------------------
+    host_tree = tree.to_host()
+    xh = torch.randn(k, n, dtype=torch.float64).pin_memory()
+    yh = torch.zeros(k, n, dtype=torch.float64).pin_memory()
+    ierr = C.c_int(0)
+    xp = C.cast(C.c_void_p(xh.data_ptr()), abi.DP)
+    yp = C.cast(C.c_void_p(yh.data_ptr()), abi.DP)
+    for _ in range(max(1, args.warmup)):
+        lib.multiply_hodlr_dense(host_tree.tp, xp, k, n, yp, n, C.byref(ierr))
+    assert ierr.value == 0
+    e2e_steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        lib.multiply_hodlr_dense(host_tree.tp, xp, k, n, yp, n, C.byref(ierr))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if pg:
+        t = torch.tensor([e2e_s], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = t.item()
+    e2e = bytes_step * world / e2e_s / 1e9
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel (phase 2: output bands) --------------------
+    p1_ms, p2_ms, cnt = pt[0] / max(pt[2], 1), pt[1] / max(pt[2], 1), pt[2]
+    # phase 2 streams every leaf and U factor once and writes Y: its algorithmic
+    # work is 2 k (sum m_leaf^2 + sum s m) flops; phase 1 is 2 k sum s n
+    peak = fp64_peak_tflops(torch, dev)
+    dom = "phase2" if p2_ms >= p1_ms else "phase1"
+    n_leaf = 1 << h
+    leaf = n // n_leaf
+    leaves_el = n_leaf * leaf * leaf
+    lowrank_el = storage - leaves_el
+    p2_flops = 2.0 * k * (leaves_el + lowrank_el / 2.0)
+    p1_flops = 2.0 * k * (lowrank_el / 2.0)
+    dom_flops, dom_ms = (p2_flops, p2_ms) if dom == "phase2" else (p1_flops, p1_ms)
+    achieved = dom_flops / (dom_ms * 1e-3) / 1e12
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        res = run_cpu_baseline(args.cpu_n, k)
+        if "error" not in res:
+            cpu = {"value": res["matmat_gbs"], "unit": "GB/s", "cores": res["threads"],
+                   "kind": "reference",
+                   "sample": f"hmat_lib multiply_hodlr_dense k={k} on its own build at "
+                             f"n={res['n']} (same kernel family; build {res['build_s']:.2f} s)",
+                   "build_s": res["build_s"], "cpu": res.get("cpu")}
+        else:
+            cpu = {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "failed: " + res["error"]}
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "precision": "fp64",
+        "config": {"workload": WORKLOAD, "n": n, "height": h, "leaf": n // (1 << h), "k": k,
+                   "tol": tol, "kernel": "matern32 l=0.1 +1e-2 I, 2D Morton points seed 1",
+                   "l2": "inputs larger than L2 (factors + X > 126 MB), no flush",
+                   "parallelism": f"replicas{world}"},
+        "build_s": build_s,
+        "rel_err_vs_dense": rel_err,
+        "tree": {"max_rank": info["max_rank"], "storage_doubles": storage,
+                 "ranks_by_depth": [int(max(ranks[2 * ((1 << d) - 1):2 * ((1 << (d + 1)) - 1)]))
+                                    for d in range(h)]},
+        "gflops": flops_step / (ms_step * 1e-3) / 1e9,
+        "roofline": {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                     "phase_ms": {"phase1": p1_ms, "phase2": p2_ms}},
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": int(8 * n * k),
+                "d2h_bytes_per_step": int(8 * n * k), "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": int(launches),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    host_tree.free()
+    tree.free()
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

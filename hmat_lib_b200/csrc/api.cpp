@@ -31,7 +31,8 @@ int fail(int *ierr, const Error &e) {
   return e.code;
 }
 
-cudaStream_t as_stream(void *s) { return s ? (cudaStream_t)s : lib_stream(); }
+// NULL selects the CUDA default stream, as CUDA libraries do.
+cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
 
 // Leaf sizes of a tree of height h over m rows with halving splits, the
 // top-left child taking m - m/2 (hmat_lib src/constructors.c:60-64).
@@ -454,6 +455,8 @@ int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshol
     return fail(ierr, e);
   }
 }
+
+int hodlr_b200_phase_times(double *out, int capacity) { return phase_times(out, capacity); }
 
 int hodlr_b200_sync_tree(const TreeHODLR *hodlr) {
   try {

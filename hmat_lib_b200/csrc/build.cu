@@ -1,15 +1,58 @@
 // Dense -> HODLR construction (replaces hmat_lib src/constructors.c:629-704:
 // copy_diagonal_blocks :212, compress_matrix :449, compress_off_diagonal
-// :308).  Off-diagonal blocks of all levels are disjoint, so every block of
-// every level is compressed in the same batched launches (the reference
-// walks levels bottom-up with one OpenMP task per block).
+// :308, svd_double src/lapack_wrapper.c:8).
+//
+// Off-diagonal blocks of all levels are disjoint, so every block of every
+// level is compressed in the same batched launches (the reference walks the
+// levels bottom-up with one OpenMP task per block).  Two paths:
+//
+//  * exact: min(m, n) <= exact_max -> one-sided Jacobi SVD of the block;
+//  * sketched: adaptive blocked randomized range finder.  Each round draws a
+//    Gaussian test matrix Om, forms Y = A Om - Q (B Om) with one pass over
+//    the block, orthonormalises Y panel by panel against the basis Q (block
+//    classical Gram-Schmidt applied twice, then TSQR), and appends
+//    B^T = A^T Q_new with a second pass.  The columns of B^T are in turn
+//    orthonormalised into P with their coefficients collected in R_B, so
+//    A ~ Q R_B^T P^T.  A round stops adding columns once the residual norm
+//    estimated from the newest panel, ||(I - QQ^T) A Om_p||_F / sqrt(w),
+//    falls below eta * tol * (a lower bound of sigma_0).  A Jacobi SVD of the
+//    small R_B^T then gives the singular values; the rank follows hmat_lib's
+//    relative rule and U = Q U_R Sigma, V = P V_R.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 
 #include "build.h"
 #include "jacobi.h"
+#include "tsqr.h"
 
 namespace hb {
+
+namespace {
+
+enum GB { kA = 0, kWork = 1, kArena = 2 };
+
+template <class T>
+T *upload_vec(const std::vector<T> &v, cudaStream_t s) {
+  T *d = nullptr;
+  HB_CUDA(cudaMallocAsync((void **)&d, sizeof(T) * std::max<size_t>(v.size(), 1), s));
+  if (!v.empty())
+    HB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+struct SketchBlock {
+  int b;                 // block index in the geometry
+  int m, n, cap;
+  long long a_off;       // offset of the block in the input (base kA)
+  long long q, bt, p, rb, om, t, c, rn;   // offsets in the work buffer
+  int ell = 0;
+  bool done = false;
+  double sig_lb = 0.0;   // lower bound of sigma_0: largest row norm of B
+  int last_pw = 0;
+};
+
+}  // namespace
 
 std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double *d_A,
                                              long long lda, double tol, cudaStream_t stream,
@@ -18,104 +61,401 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   Geometry g = g_in;
   const int nb = g.nblock();
   *svd_status = SUCCESS;
+  const int exact_max = (int)option("exact_max", 128);
+  const int cap_max = (int)option("sketch_cap", 1024) / kPanel * kPanel;
+  const int w_first = std::max(kPanel, (int)option("sketch_first", 64) / kPanel * kPanel);
+  const int w_next = std::max(kPanel, (int)option("sketch_step", 64) / kPanel * kPanel);
+  const double eta = option("sketch_eta", 0.01);
+  const unsigned long long seed = (unsigned long long)option("sketch_seed", 20240607);
 
-  // ---- exact path: one Jacobi SVD per block --------------------------------
-  std::vector<JacobiProb> probs;
-  std::vector<int> prob_block;
-  long long scratch = 0;
-  int max_c = 0;
-  struct Slots { long long ws, u, v, sig; };
-  std::vector<Slots> slots;
+  // ---- partition the blocks --------------------------------------------------
+  std::vector<int> exact, sketched;
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
     const int C = std::min(B.m, B.n);
     if (C == 0) continue;
-    Slots s;
-    s.ws = scratch;
-    scratch += jacobi_workspace(B.m, B.n);
-    s.u = scratch;
-    scratch += align_up((long long)B.m * C);
-    s.v = scratch;
-    scratch += align_up((long long)B.n * C);
-    s.sig = scratch;
-    scratch += align_up(C);
-    slots.push_back(s);
-    prob_block.push_back(b);
+    (C <= exact_max ? exact : sketched).push_back(b);
+  }
+
+  // ---- scratch layout ----------------------------------------------------------
+  long long scratch = 0;
+  auto take = [&](long long elems) {
+    const long long o = scratch;
+    scratch += align_up(std::max<long long>(elems, 1));
+    return o;
+  };
+  struct ExactSlot { long long ws, u, v, sig; };
+  std::vector<ExactSlot> eslots;
+  int max_c = 0;
+  for (int b : exact) {
+    const BlockDesc &B = g.blocks[b];
+    const int C = std::min(B.m, B.n);
+    ExactSlot s;
+    s.ws = take(jacobi_workspace(B.m, B.n));
+    s.u = take((long long)B.m * C);
+    s.v = take((long long)B.n * C);
+    s.sig = take(C);
+    eslots.push_back(s);
     max_c = std::max(max_c, C);
   }
-  const int np = (int)prob_block.size();
+  std::vector<SketchBlock> sk;
+  const int w_max = std::max(w_first, w_next);
+  for (int b : sketched) {
+    const BlockDesc &B = g.blocks[b];
+    SketchBlock S;
+    S.b = b;
+    S.m = B.m;
+    S.n = B.n;
+    S.cap = std::min(std::min(B.m, B.n), std::max(cap_max, kPanel));
+    S.a_off = B.r0 + (long long)B.c0 * lda;
+    S.q = take((long long)B.m * S.cap);
+    S.bt = take((long long)B.n * S.cap);
+    S.p = take((long long)B.n * S.cap);
+    S.rb = take((long long)S.cap * S.cap);
+    S.om = take((long long)B.n * w_max);
+    S.t = take((long long)S.cap * w_max);
+    S.c = take((long long)S.cap * kPanel);
+    S.rn = take((long long)kPanel * kPanel + w_max);
+    sk.push_back(S);
+  }
   double *work = dev_alloc(scratch, stream);
-  int *d_rank = nullptr, *d_status = nullptr;
-  JacobiProb *d_probs = nullptr;
-  HB_CUDA(cudaMallocAsync((void **)&d_rank, sizeof(int) * (np + 1), stream));
-  d_status = d_rank + np;
-  HB_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), stream));
-  for (int p = 0; p < np; ++p) {
-    const BlockDesc &B = g.blocks[prob_block[p]];
+  GemmBases bases{};
+  bases.p[kA] = const_cast<double *>(d_A);
+  bases.p[kWork] = work;
+  for (int i = 2; i < kGemmBases; ++i) bases.p[i] = work;
+  if (!sk.empty()) HB_CUDA(cudaMemsetAsync(work, 0, scratch * sizeof(double), stream));
+
+  int *d_int = nullptr;   // ranks of exact blocks, ranks of sketched blocks, status
+  const int n_int = (int)exact.size() + (int)sk.size() + 1;
+  HB_CUDA(cudaMallocAsync((void **)&d_int, sizeof(int) * n_int, stream));
+  HB_CUDA(cudaMemsetAsync(d_int, 0, sizeof(int) * n_int, stream));
+  int *d_status = d_int + n_int - 1;
+  JacobiParams prm;
+  prm.tol = tol;
+  prm.trunc = Truncation::Relative;
+  prm.scale_u = 1;
+  prm.max_sweeps = (int)option("jacobi_max_sweeps", 60);
+
+  // ---- exact path ----------------------------------------------------------------
+  std::vector<JacobiProb> eprobs;
+  for (size_t p = 0; p < exact.size(); ++p) {
+    const BlockDesc &B = g.blocks[exact[p]];
     const int R = std::max(B.m, B.n), C = std::min(B.m, B.n);
-    JacobiProb jp;
+    JacobiProb jp{};
     jp.A = d_A + B.r0 + (long long)B.c0 * lda;
     jp.lda = lda;
+    jp.transA = 0;
     jp.m = B.m;
     jp.n = B.n;
-    jp.G = work + slots[p].ws;
+    jp.G = work + eslots[p].ws;
     jp.W = jp.G + align_up((long long)R * C);
-    jp.U = work + slots[p].u;
+    jp.U = work + eslots[p].u;
     jp.ldu = B.m;
-    jp.V = work + slots[p].v;
+    jp.V = work + eslots[p].v;
     jp.ldv = B.n;
-    jp.sigma = work + slots[p].sig;
-    jp.rank = d_rank + p;
-    probs.push_back(jp);
+    jp.sigma = work + eslots[p].sig;
+    jp.rank = d_int + p;
+    eprobs.push_back(jp);
   }
-  if (np) {
-    HB_CUDA(cudaMallocAsync((void **)&d_probs, sizeof(JacobiProb) * np, stream));
-    HB_CUDA(cudaMemcpyAsync(d_probs, probs.data(), sizeof(JacobiProb) * np,
-                            cudaMemcpyHostToDevice, stream));
-    JacobiParams prm;
-    prm.tol = tol;
-    prm.trunc = Truncation::Relative;
-    prm.scale_u = 1;
-    prm.max_sweeps = (int)option("jacobi_max_sweeps", 60);
-    jacobi_svd_batched(d_probs, np, prm, d_status, max_c, stream);
+  JacobiProb *d_eprobs = nullptr;
+  if (!eprobs.empty()) {
+    d_eprobs = upload_vec(eprobs, stream);
+    jacobi_svd_batched(d_eprobs, (int)eprobs.size(), prm, d_status, max_c, stream);
   }
-  std::vector<int> ranks(np + 1, 0);
-  HB_CUDA(cudaMemcpyAsync(ranks.data(), d_rank, sizeof(int) * (np + 1), cudaMemcpyDeviceToHost,
+
+  // ---- sketched path ---------------------------------------------------------------
+  int rounds = 0;
+  bool cap_hit = false;
+  std::vector<double> host_rn;
+  while (true) {
+    std::vector<int> act;
+    for (size_t i = 0; i < sk.size(); ++i)
+      if (!sk[i].done) act.push_back((int)i);
+    if (act.empty()) break;
+    const int wr = rounds == 0 ? w_first : w_next;
+    std::vector<int> wb(sk.size(), 0);
+    for (int i : act) {
+      wb[i] = std::min(wr, sk[i].cap - sk[i].ell);
+      if (wb[i] <= 0) {
+        sk[i].done = true;
+        cap_hit = true;
+      }
+    }
+    act.erase(std::remove_if(act.begin(), act.end(), [&](int i) { return wb[i] <= 0; }),
+              act.end());
+    if (act.empty()) break;
+
+    // 1. Gaussian test matrices
+    std::vector<RandDesc> rd;
+    for (int i : act)
+      rd.push_back(RandDesc{work + sk[i].om, sk[i].n, sk[i].n, wb[i],
+                            ((unsigned long long)sk[i].b << 24) + (unsigned long long)rounds});
+    gaussian_fill(rd, seed, stream);
+
+    // 2. Y = A Om written into the new columns of Q; 3. Y -= Q (B Om)
+    {
+      GemmBatch g1;
+      for (int i : act) {
+        const SketchBlock &S = sk[i];
+        int pr = g1.add(kWork, S.q + (long long)S.ell * S.m, S.m, S.m, wb[i]);
+        g1.seg(pr, kA, S.a_off, lda, 0, kWork, S.om, S.n, 0, S.n);
+      }
+      gemm_f64_run(g1, bases, TileShape::M128N64, stream);
+      GemmBatch g2;
+      for (int i : act) {
+        const SketchBlock &S = sk[i];
+        if (S.ell == 0) continue;
+        int pr = g2.add(kWork, S.t, S.ell, S.ell, wb[i]);
+        g2.seg(pr, kWork, S.bt, S.n, 1, kWork, S.om, S.n, 0, S.n);
+      }
+      gemm_f64_run(g2, bases, TileShape::M64N128, stream);
+      GemmBatch g3;
+      for (int i : act) {
+        const SketchBlock &S = sk[i];
+        if (S.ell == 0) continue;
+        int pr = g3.add(kWork, S.q + (long long)S.ell * S.m, S.m, S.m, wb[i], -1.0, 1.0);
+        g3.seg(pr, kWork, S.q, S.m, 0, kWork, S.t, S.ell, 0, S.ell);
+      }
+      gemm_f64_run(g3, bases, TileShape::M128N64, stream, false);
+    }
+
+    // 4. panel-wise orthonormalisation of the new Q columns (BCGS2 + TSQR)
+    auto orthonormalise = [&](bool left) {
+      int max_panels = 0;
+      for (int i : act) max_panels = std::max(max_panels, (wb[i] + kPanel - 1) / kPanel);
+      for (int q = 0; q < max_panels; ++q) {
+        std::vector<int> pa;
+        for (int i : act)
+          if (q * kPanel < wb[i]) pa.push_back(i);
+        for (int rep = 0; rep < 2; ++rep) {
+          GemmBatch gc, gu;
+          std::vector<CopyDesc> acc;
+          for (int i : pa) {
+            const SketchBlock &S = sk[i];
+            const int p0 = S.ell + q * kPanel, pw = std::min(kPanel, wb[i] - q * kPanel);
+            if (p0 == 0) continue;
+            const int rows = left ? S.m : S.n;
+            const long long base = left ? S.q : S.p;
+            const long long panel = base + (long long)p0 * rows;
+            // C (p0 x pw) = Base[:, :p0]^T Panel
+            const long long cdst = left ? S.c : S.rb + (long long)p0 * S.cap;
+            const long long cld = left ? S.cap : S.cap;
+            const long long ctarget = (!left && rep == 0) ? cdst : S.c;
+            int pr = gc.add(kWork, ctarget, left ? S.cap : cld, p0, pw);
+            gc.seg(pr, kWork, base, rows, 1, kWork, panel, rows, 0, rows);
+            // Panel -= Base[:, :p0] C
+            int pu = gu.add(kWork, panel, rows, rows, pw, -1.0, 1.0);
+            gu.seg(pu, kWork, base, rows, 0, kWork, ctarget, left ? S.cap : cld, 0, p0);
+            if (!left && rep == 1)
+              acc.push_back(CopyDesc{work + S.c, S.cap, work + cdst, S.cap, p0, pw});
+          }
+          gemm_f64_run(gc, bases, TileShape::M64N128, stream);
+          gemm_f64_run(gu, bases, TileShape::M128N64, stream, false);
+          if (!acc.empty()) {
+            CopyDesc *d = upload_vec(acc, stream);
+            add2d_batched(d, (int)acc.size(), 1.0, stream);
+            cudaFreeAsync(d, stream);
+          }
+        }
+        std::vector<TsqrProb> tp;
+        for (int i : pa) {
+          const SketchBlock &S = sk[i];
+          const int p0 = S.ell + q * kPanel, pw = std::min(kPanel, wb[i] - q * kPanel);
+          const int rows = left ? S.m : S.n;
+          const long long base = left ? S.q : S.p;
+          TsqrProb t;
+          t.Y = work + base + (long long)p0 * rows;
+          t.ldy = rows;
+          t.m = rows;
+          t.w = pw;
+          if (left) {
+            t.R = work + S.rn;
+            t.ldr = kPanel;
+          } else {
+            t.R = work + S.rb + p0 + (long long)p0 * S.cap;
+            t.ldr = S.cap;
+          }
+          tp.push_back(t);
+          if (left) sk[i].last_pw = pw;
+        }
+        tsqr_batched(tp, stream);
+      }
+    };
+    orthonormalise(true);
+
+    // residual estimate of the last panel: ||R_last||_F^2
+    {
+      std::vector<NormDesc> nd;
+      for (int i : act)
+        nd.push_back(NormDesc{work + sk[i].rn, kPanel, sk[i].last_pw, sk[i].last_pw,
+                              work + sk[i].rn + kPanel * kPanel});
+      column_norms2(nd, stream);
+    }
+
+    // 5. B^T new columns = A^T Q_new; copy them to P for orthonormalisation
+    {
+      GemmBatch g5;
+      for (int i : act) {
+        const SketchBlock &S = sk[i];
+        int pr = g5.add(kWork, S.bt + (long long)S.ell * S.n, S.n, S.n, wb[i]);
+        g5.seg(pr, kA, S.a_off, lda, 1, kWork, S.q + (long long)S.ell * S.m, S.m, 0, S.m);
+      }
+      gemm_f64_run(g5, bases, TileShape::M128N64, stream);
+      std::vector<CopyDesc> cp;
+      for (int i : act) {
+        const SketchBlock &S = sk[i];
+        cp.push_back(CopyDesc{work + S.bt + (long long)S.ell * S.n, S.n,
+                              work + S.p + (long long)S.ell * S.n, S.n, S.n, wb[i]});
+      }
+      CopyDesc *d = upload_vec(cp, stream);
+      copy2d_batched(d, (int)cp.size(), stream);
+      cudaFreeAsync(d, stream);
+    }
+    // 6. P / R_B update
+    orthonormalise(false);
+
+    // 7. row norms of the new rows of B (= column norms of B^T)
+    {
+      std::vector<NormDesc> nd;
+      for (int i : act) {
+        const SketchBlock &S = sk[i];
+        nd.push_back(NormDesc{work + S.bt + (long long)S.ell * S.n, S.n, S.n, wb[i],
+                              work + S.t});
+      }
+      column_norms2(nd, stream);
+    }
+    // 8. read back and decide
+    std::vector<double> bn(act.size() * w_max, 0.0), rcols(act.size() * kPanel, 0.0);
+    for (size_t a = 0; a < act.size(); ++a) {
+      const SketchBlock &S = sk[act[a]];
+      HB_CUDA(cudaMemcpyAsync(&bn[a * w_max], work + S.t, sizeof(double) * wb[act[a]],
+                              cudaMemcpyDeviceToHost, stream));
+      HB_CUDA(cudaMemcpyAsync(&rcols[a * kPanel], work + S.rn + kPanel * kPanel,
+                              sizeof(double) * S.last_pw, cudaMemcpyDeviceToHost, stream));
+    }
+    HB_CUDA(cudaStreamSynchronize(stream));
+    for (size_t a = 0; a < act.size(); ++a) {
+      SketchBlock &S = sk[act[a]];
+      double f2 = 0.0;
+      for (int c = 0; c < S.last_pw; ++c) f2 += rcols[a * kPanel + c];
+      for (int c = 0; c < wb[act[a]]; ++c) S.sig_lb = std::max(S.sig_lb, std::sqrt(bn[a * w_max + c]));
+      S.ell += wb[act[a]];
+      const double res = std::sqrt(f2 / std::max(S.last_pw, 1));
+      // stop at the tolerance, or at the FP64 noise floor of the estimate
+      const double floor_rel = std::max(eta * tol, 1e-14);
+      if (S.ell >= std::min(S.m, S.n) || S.sig_lb == 0.0 || res <= floor_rel * S.sig_lb)
+        S.done = true;
+    }
+    ++rounds;
+  }
+
+  // ---- SVD of R_B^T for the sketched blocks ------------------------------------------
+  std::vector<JacobiProb> sprobs;
+  std::vector<long long> s_u(sk.size()), s_v(sk.size());
+  int max_l = 0;
+  long long jscratch = 0;
+  for (size_t i = 0; i < sk.size(); ++i) {
+    const int L = sk[i].ell;
+    max_l = std::max(max_l, L);
+    jscratch += jacobi_workspace(L, L) + 2 * align_up((long long)L * L) + align_up(L);
+  }
+  double *jwork = sk.empty() ? nullptr : dev_alloc(jscratch, stream);
+  {
+    long long o = 0;
+    for (size_t i = 0; i < sk.size(); ++i) {
+      const SketchBlock &S = sk[i];
+      const int L = S.ell;
+      JacobiProb jp{};
+      jp.A = work + S.rb;
+      jp.lda = S.cap;
+      jp.transA = 1;
+      jp.m = L;
+      jp.n = L;
+      jp.G = jwork + o;
+      jp.W = jp.G + align_up((long long)L * L);
+      o += jacobi_workspace(L, L);
+      jp.U = jwork + o;
+      s_u[i] = o;
+      jp.ldu = L;
+      o += align_up((long long)L * L);
+      jp.V = jwork + o;
+      s_v[i] = o;
+      jp.ldv = L;
+      o += align_up((long long)L * L);
+      jp.sigma = jwork + o;
+      o += align_up(L);
+      jp.rank = d_int + exact.size() + i;
+      sprobs.push_back(jp);
+    }
+  }
+  JacobiProb *d_sprobs = nullptr;
+  if (!sprobs.empty()) {
+    d_sprobs = upload_vec(sprobs, stream);
+    jacobi_svd_batched(d_sprobs, (int)sprobs.size(), prm, d_status, max_l, stream);
+  }
+  std::vector<int> ints(n_int, 0);
+  HB_CUDA(cudaMemcpyAsync(ints.data(), d_int, sizeof(int) * n_int, cudaMemcpyDeviceToHost,
                           stream));
   HB_CUDA(cudaStreamSynchronize(stream));
-  *svd_status = ranks[np];
+  *svd_status = ints[n_int - 1];
   for (auto &B : g.blocks) B.s = 0;
-  for (int p = 0; p < np; ++p) g.blocks[prob_block[p]].s = ranks[p];
+  for (size_t p = 0; p < exact.size(); ++p) g.blocks[exact[p]].s = ints[p];
+  for (size_t i = 0; i < sk.size(); ++i) g.blocks[sk[i].b].s = ints[exact.size() + i];
 
-  // ---- arena: leaves copied from the input, factors from the scratch -------
+  // ---- arena: leaves from the input, factors from the scratch ------------------------
   std::shared_ptr<DeviceTree> dt = dtree_create(g, stream);
   std::vector<CopyDesc> copies;
   for (int i = 0; i < g.nleaf(); ++i) {
     const LeafDesc &L = dt->leaves[i];
     if (L.m == 0) continue;
-    copies.push_back(CopyDesc{d_A + L.r0 + (long long)L.r0 * lda, lda, dt->arena + L.off, L.m,
-                              L.m, L.m});
+    copies.push_back(
+        CopyDesc{d_A + L.r0 + (long long)L.r0 * lda, lda, dt->arena + L.off, L.m, L.m, L.m});
   }
-  for (int p = 0; p < np; ++p) {
-    const BlockDesc &B = dt->g.blocks[prob_block[p]];
+  for (size_t p = 0; p < exact.size(); ++p) {
+    const BlockDesc &B = dt->g.blocks[exact[p]];
     if (B.s == 0) continue;
-    copies.push_back(CopyDesc{probs[p].U, B.m, dt->arena + B.u_off, B.m, B.m, B.s});
-    copies.push_back(CopyDesc{probs[p].V, B.n, dt->arena + B.v_off, B.n, B.n, B.s});
+    copies.push_back(CopyDesc{eprobs[p].U, B.m, dt->arena + B.u_off, B.m, B.m, B.s});
+    copies.push_back(CopyDesc{eprobs[p].V, B.n, dt->arena + B.v_off, B.n, B.n, B.s});
   }
   if (!copies.empty()) {
-    CopyDesc *d_copies = nullptr;
-    HB_CUDA(cudaMallocAsync((void **)&d_copies, sizeof(CopyDesc) * copies.size(), stream));
-    HB_CUDA(cudaMemcpyAsync(d_copies, copies.data(), sizeof(CopyDesc) * copies.size(),
-                            cudaMemcpyHostToDevice, stream));
-    copy2d_batched(d_copies, (int)copies.size(), stream);
-    dev_free(d_copies, stream);
+    CopyDesc *d = upload_vec(copies, stream);
+    copy2d_batched(d, (int)copies.size(), stream);
+    cudaFreeAsync(d, stream);
   }
-  dev_free(d_probs, stream);
-  dev_free(d_rank, stream);
+  if (!sk.empty()) {
+    // U = Q[:, :ell] (U_R Sigma)[:, :s],  V = P[:, :ell] V_R[:, :s]
+    GemmBases fb{};
+    fb.p[0] = work;
+    fb.p[1] = jwork;
+    fb.p[2] = dt->arena;
+    for (int i = 3; i < kGemmBases; ++i) fb.p[i] = work;
+    GemmBatch gf;
+    for (size_t i = 0; i < sk.size(); ++i) {
+      const SketchBlock &S = sk[i];
+      const BlockDesc &B = dt->g.blocks[S.b];
+      if (B.s == 0) continue;
+      int pu = gf.add(2, B.u_off, B.m, B.m, B.s);
+      gf.seg(pu, 0, S.q, S.m, 0, 1, s_u[i], S.ell, 0, S.ell);
+      int pv = gf.add(2, B.v_off, B.n, B.n, B.s);
+      gf.seg(pv, 0, S.p, S.n, 0, 1, s_v[i], S.ell, 0, S.ell);
+    }
+    gemm_f64_run(gf, fb, TileShape::M128N64, stream, false);
+  }
+  HB_CUDA(cudaStreamSynchronize(stream));
+  dev_free(d_eprobs, stream);
+  dev_free(d_sprobs, stream);
+  dev_free(d_int, stream);
+  dev_free(jwork, stream);
   dev_free(work, stream);
   HB_CUDA(cudaStreamSynchronize(stream));
+  if (cap_hit) {
+    *svd_status = SVD_FAILURE;
+    set_last_error("a block's rank reached the sketch cap (option sketch_cap)");
+  }
   if (stats) {
-    stats->exact_blocks = np;
+    stats->exact_blocks = (int)exact.size();
+    stats->sketched_blocks = (int)sk.size();
+    stats->sketch_rounds = rounds;
     stats->seconds =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }

@@ -45,7 +45,9 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
   double *G = P.G, *W = P.W;
   for (long long e = tid; e < (long long)R * C; e += blockDim.x) {
     const int r = (int)(e % R), c = (int)(e / R);
-    G[e] = tall ? P.A[r + (long long)c * P.lda] : P.A[c + (long long)r * P.lda];
+    // logical element (i, j) of the m x n input
+    const int i = tall ? r : c, j = tall ? c : r;
+    G[e] = P.transA ? P.A[j + (long long)i * P.lda] : P.A[i + (long long)j * P.lda];
   }
   for (long long e = tid; e < (long long)C * C; e += blockDim.x)
     W[e] = ((e % C) == (e / C)) ? 1.0 : 0.0;
@@ -179,6 +181,16 @@ __global__ void copy2d_kernel(const CopyDesc *__restrict__ descs) {
   }
 }
 
+__global__ void add2d_kernel(const CopyDesc *__restrict__ descs, double alpha) {
+  const CopyDesc D = descs[blockIdx.y];
+  const long long total = (long long)D.rows * D.cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e % D.rows, c = e / D.rows;
+    D.dst[r + c * D.ldd] += alpha * D.src[r + c * D.lds];
+  }
+}
+
 }  // namespace
 
 void jacobi_svd_batched(const JacobiProb *d_probs, int nprobs, const JacobiParams &prm,
@@ -202,4 +214,15 @@ void copy2d_batched(const CopyDesc *d_descs, int n, cudaStream_t stream) {
   }
 }
 
+}  // namespace hb
+
+namespace hb {
+void add2d_batched(const CopyDesc *d_descs, int n, double alpha, cudaStream_t stream) {
+  if (n <= 0) return;
+  for (int off = 0; off < n; off += 65535) {
+    dim3 grid(32, std::min(65535, n - off));
+    add2d_kernel<<<grid, 256, 0, stream>>>(d_descs + off, alpha);
+    HB_LAUNCHED();
+  }
+}
 }  // namespace hb

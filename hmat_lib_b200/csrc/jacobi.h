@@ -10,8 +10,9 @@ namespace hb {
 // columns of the tall orientation in G (R x C, ld R) while accumulating the
 // rotations in W (C x C, ld C).
 struct JacobiProb {
-  const double *A;
+  const double *A;  // element (i, j) at A[i + j lda], or A[j + i lda] if transA
   long long lda;
+  int transA;
   int m, n;
   double *G;        // workspace R x C
   double *W;        // workspace C x C
@@ -59,5 +60,8 @@ struct CopyDesc {
 };
 
 void copy2d_batched(const CopyDesc *d_descs, int n, cudaStream_t stream);
+
+// dst += alpha * src for every descriptor (same shape rules as CopyDesc).
+void add2d_batched(const CopyDesc *d_descs, int n, double alpha, cudaStream_t stream);
 
 }  // namespace hb

@@ -115,6 +115,45 @@ ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long l
   return ref;
 }
 
+// Optional per-phase timing: with option "record_phase_times" set, events are
+// recorded on the launching stream around each phase and their elapsed times
+// accumulated (read and reset with hodlr_b200_phase_times).  Work is never
+// skipped; the events only bracket it.
+namespace {
+std::mutex g_pt_mutex;
+struct PhaseEvents {
+  cudaEvent_t e[3];
+};
+std::vector<PhaseEvents> g_pending;
+double g_phase_ms[2] = {0.0, 0.0};
+long long g_phase_count = 0;
+
+void collect_phase_times() {
+  for (auto &pe : g_pending) {
+    cudaEventSynchronize(pe.e[2]);
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, pe.e[0], pe.e[1]);
+    cudaEventElapsedTime(&b, pe.e[1], pe.e[2]);
+    g_phase_ms[0] += a;
+    g_phase_ms[1] += b;
+    g_phase_count += 1;
+    for (auto ev : pe.e) cudaEventDestroy(ev);
+  }
+  g_pending.clear();
+}
+}  // namespace
+
+int phase_times(double *out, int cap) {
+  std::lock_guard<std::mutex> lk(g_pt_mutex);
+  collect_phase_times();
+  if (cap >= 1 && out) out[0] = g_phase_ms[0];
+  if (cap >= 2 && out) out[1] = g_phase_ms[1];
+  if (cap >= 3 && out) out[2] = (double)g_phase_count;
+  g_phase_ms[0] = g_phase_ms[1] = 0.0;
+  g_phase_count = 0;
+  return 3;
+}
+
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
                  long long ldy, cudaStream_t stream) {
   if (k <= 0 || t.g.n == 0) return;
@@ -126,8 +165,20 @@ void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx
   bases.p[kW] = plan.w;
   bases.p[4] = t.arena;
   bases.p[5] = t.arena;
+  const bool timed = option("record_phase_times", 0.0) != 0.0;
+  PhaseEvents pe{};
+  if (timed) {
+    for (auto &ev : pe.e) HB_CUDA(cudaEventCreate(&ev));
+    HB_CUDA(cudaEventRecord(pe.e[0], stream));
+  }
   gemm_plan_run(plan.phase1, bases, stream);
+  if (timed) HB_CUDA(cudaEventRecord(pe.e[1], stream));
   gemm_plan_run(plan.phase2, bases, stream);
+  if (timed) {
+    HB_CUDA(cudaEventRecord(pe.e[2], stream));
+    std::lock_guard<std::mutex> lk(g_pt_mutex);
+    g_pending.push_back(pe);
+  }
 }
 
 }  // namespace hb

@@ -45,6 +45,11 @@ ProductWork product_work(const DeviceTree &t, int k);
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
                  long long ldy, cudaStream_t stream);
 
+// Accumulated per-phase device times (ms) of products run with option
+// "record_phase_times" set: out[0] phase 1, out[1] phase 2, out[2] count.
+// Resets the accumulators.
+int phase_times(double *out, int cap);
+
 // Builds (and caches on the tree) the plan for this shape without running it.
 ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,
                           cudaStream_t stream);

@@ -1,0 +1,345 @@
+// Batched TSQR (Householder QR of 256-row chunks in shared memory, reduced
+// up a tree of stacked R factors, explicit Q rebuilt top-down) plus the
+// small utility kernels of the randomized compression: Gaussian test
+// matrices, column norms.
+//
+// Replaces the dgeqrt factorisations of hmat_lib (src/hodlr_algebra.c:120,
+// 126) and provides the orthonormal bases of the randomized range finder
+// that stands in for dgesdd on large blocks (src/constructors.c:323).
+#include <algorithm>
+
+#include "tsqr.h"
+
+namespace hb {
+
+namespace {
+
+constexpr int kQT = 256;   // threads per CTA (one row of a chunk each)
+
+struct QrChunk {
+  double *A;
+  long long lda;
+  int rows, w;
+  double *R;
+  long long ldr;
+};
+
+struct MulChunk {
+  double *Q;
+  long long ldq;
+  int rows, w;
+  const double *M;
+  long long ldm;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kQT / 32; ++k) s += red[k];
+  __syncthreads();
+  return s;
+}
+
+constexpr size_t kQrSmem = sizeof(double) * (2 * kChunk * kPanel + 2 * kPanel + kQT / 32);
+
+// Householder QR of one chunk (rows <= 256, w <= 32), LAPACK dlarfg
+// convention: H_j = I - tau_j v_j v_j^T, v_j(j) = 1, beta_j = -sign(x0)||x||.
+__global__ void __launch_bounds__(kQT) qr_chunk_kernel(const QrChunk *__restrict__ descs) {
+  const QrChunk D = descs[blockIdx.x];
+  extern __shared__ double sm[];
+  double *S = sm;                          // chunk, column-major, ld kChunk
+  double *E = S + kChunk * kPanel;         // explicit Q under construction
+  double *tau = E + kChunk * kPanel;
+  double *wv = tau + kPanel;
+  double *red = wv + kPanel;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r = D.rows, w = D.w, k = min(r, w);
+
+  for (int e = tid; e < kChunk * kPanel; e += kQT) {
+    const int i = e % kChunk, j = e / kChunk;
+    S[e] = (i < r && j < w) ? D.A[i + (long long)j * D.lda] : 0.0;
+  }
+  __syncthreads();
+
+  for (int j = 0; j < k; ++j) {
+    double part = 0.0;
+    for (int i = j + 1 + tid; i < r; i += kQT) part = fma(S[i + j * kChunk], S[i + j * kChunk], part);
+    const double sigma2 = block_sum(part, red);
+    const double x0 = S[j + j * kChunk];
+    double beta = x0, t = 0.0, scale = 0.0;
+    if (sigma2 > 0.0) {
+      const double nrm = sqrt(fma(x0, x0, sigma2));
+      beta = x0 >= 0.0 ? -nrm : nrm;
+      t = (beta - x0) / beta;
+      scale = 1.0 / (x0 - beta);
+    }
+    __syncthreads();
+    for (int i = j + 1 + tid; i < r; i += kQT) S[i + j * kChunk] *= scale;
+    if (tid == 0) {
+      S[j + j * kChunk] = beta;
+      tau[j] = t;
+    }
+    __syncthreads();
+    for (int c = j + 1 + warp; c < w; c += kQT / 32) {
+      double dot = lane == 0 ? S[j + c * kChunk] : 0.0;
+      for (int i = j + 1 + lane; i < r; i += 32) dot = fma(S[i + j * kChunk], S[i + c * kChunk], dot);
+      dot = warp_sum(dot);
+      if (lane == 0) wv[c] = dot * t;
+    }
+    __syncthreads();
+    const int nr = r - j, nc = w - j - 1;
+    for (int idx = tid; idx < nr * nc; idx += kQT) {
+      const int i = j + idx % nr, c = j + 1 + idx / nr;
+      const double vi = (i == j) ? 1.0 : S[i + j * kChunk];
+      S[i + c * kChunk] -= vi * wv[c];
+    }
+    __syncthreads();
+  }
+
+  // R (w x w): upper triangle of the first k rows
+  for (int e = tid; e < w * w; e += kQT) {
+    const int i = e % w, c = e / w;
+    D.R[i + (long long)c * D.ldr] = (i <= c && i < k) ? S[i + c * kChunk] : 0.0;
+  }
+  // explicit Q = H_0 ... H_{k-1} [I; 0]
+  for (int e = tid; e < kChunk * kPanel; e += kQT) {
+    const int i = e % kChunk, c = e / kChunk;
+    E[e] = (i == c && i < r && c < w) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int j = k - 1; j >= 0; --j) {
+    const double t = tau[j];
+    for (int c = j + warp; c < w; c += kQT / 32) {
+      double dot = lane == 0 ? E[j + c * kChunk] : 0.0;
+      for (int i = j + 1 + lane; i < r; i += 32) dot = fma(S[i + j * kChunk], E[i + c * kChunk], dot);
+      dot = warp_sum(dot);
+      if (lane == 0) wv[c] = dot * t;
+    }
+    __syncthreads();
+    const int nr = r - j, nc = w - j;
+    for (int idx = tid; idx < nr * nc; idx += kQT) {
+      const int i = j + idx % nr, c = j + idx / nr;
+      const double vi = (i == j) ? 1.0 : S[i + j * kChunk];
+      E[i + c * kChunk] -= vi * wv[c];
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < r * w; e += kQT) {
+    const int i = e % r, c = e / r;
+    D.A[i + (long long)c * D.lda] = E[i + c * kChunk];
+  }
+}
+
+// Q (rows x w) <- Q M (M: w x w)
+__global__ void __launch_bounds__(kQT) mul_chunk_kernel(const MulChunk *__restrict__ descs) {
+  const MulChunk D = descs[blockIdx.x];
+  __shared__ double M[kPanel * kPanel];
+  const int tid = threadIdx.x, w = D.w;
+  for (int e = tid; e < w * w; e += kQT) M[e] = D.M[(e % w) + (long long)(e / w) * D.ldm];
+  __syncthreads();
+  for (int i = tid; i < D.rows; i += kQT) {
+    double q[kPanel];
+#pragma unroll
+    for (int l = 0; l < kPanel; ++l) q[l] = l < w ? D.Q[i + (long long)l * D.ldq] : 0.0;
+    for (int c = 0; c < w; ++c) {
+      double acc = 0.0;
+#pragma unroll
+      for (int l = 0; l < kPanel; ++l) acc = fma(q[l], l < w ? M[l + c * w] : 0.0, acc);
+      D.Q[i + (long long)c * D.ldq] = acc;
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+__global__ void gaussian_kernel(const RandDesc *__restrict__ descs, unsigned long long seed) {
+  const RandDesc D = descs[blockIdx.y];
+  const unsigned long long base = splitmix64(seed ^ splitmix64(D.id + 0x632BE59BD9B4E019ULL));
+  const long long total = (long long)D.rows * D.cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long h1 = splitmix64(base + (unsigned long long)e);
+    const unsigned long long h2 = splitmix64(h1);
+    const double u1 = ((double)(h1 >> 11) + 1.0) * 0x1.0p-53;   // (0, 1]
+    const double u2 = (double)(h2 >> 11) * 0x1.0p-53;           // [0, 1)
+    const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+    const long long i = e % D.rows, j = e / D.rows;
+    D.X[i + j * D.ld] = z;
+  }
+}
+
+__global__ void colnorm_kernel(const NormDesc *__restrict__ descs) {
+  const NormDesc D = descs[blockIdx.y];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = blockIdx.x * nw + warp; c < D.cols; c += gridDim.x * nw) {
+    const double *x = D.X + (long long)c * D.ld;
+    double s = 0.0;
+    for (int i = lane; i < D.rows; i += 32) s = fma(x[i], x[i], s);
+    s = warp_sum(s);
+    if (lane == 0) D.out[c] = s;
+  }
+}
+
+template <class T>
+T *upload(const std::vector<T> &v, cudaStream_t s) {
+  T *d = nullptr;
+  HB_CUDA(cudaMallocAsync((void **)&d, sizeof(T) * std::max<size_t>(v.size(), 1), s));
+  HB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+void launch_qr(const std::vector<QrChunk> &chunks, cudaStream_t s) {
+  if (chunks.empty()) return;
+  static bool configured = false;
+  if (!configured) {
+    HB_CUDA(cudaFuncSetAttribute(qr_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kQrSmem));
+    configured = true;
+  }
+  QrChunk *d = upload(chunks, s);
+  for (size_t off = 0; off < chunks.size(); off += 65535) {
+    const int cnt = (int)std::min<size_t>(65535, chunks.size() - off);
+    qr_chunk_kernel<<<cnt, kQT, kQrSmem, s>>>(d + off);
+    HB_LAUNCHED();
+  }
+  cudaFreeAsync(d, s);
+}
+
+void launch_mul(const std::vector<MulChunk> &chunks, cudaStream_t s) {
+  if (chunks.empty()) return;
+  MulChunk *d = upload(chunks, s);
+  for (size_t off = 0; off < chunks.size(); off += 65535) {
+    const int cnt = (int)std::min<size_t>(65535, chunks.size() - off);
+    mul_chunk_kernel<<<cnt, kQT, 0, s>>>(d + off);
+    HB_LAUNCHED();
+  }
+  cudaFreeAsync(d, s);
+}
+
+}  // namespace
+
+void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t s) {
+  if (probs.empty()) return;
+  // level structure of every problem: level 0 is the panel itself, level
+  // l + 1 stacks the w x w R factors of level l's chunks
+  struct Level {
+    double *A;
+    long long lda;
+    int rows;
+    int nchunks;
+  };
+  std::vector<std::vector<Level>> levels(probs.size());
+  long long scratch = 0;
+  std::vector<std::vector<long long>> stack_off(probs.size());
+  for (size_t p = 0; p < probs.size(); ++p) {
+    const TsqrProb &P = probs[p];
+    HB_REQUIRE(P.w >= 1 && P.w <= kPanel, INPUT_ERROR, "TSQR panel wider than 32 columns");
+    int rows = P.m;
+    while (true) {
+      const int nch = std::max(1, (rows + kChunk - 1) / kChunk);
+      levels[p].push_back(Level{nullptr, 0, rows, nch});
+      if (nch == 1) break;
+      rows = nch * P.w;
+      stack_off[p].push_back(scratch);
+      scratch += align_up((long long)rows * P.w);
+    }
+  }
+  double *buf = nullptr;
+  if (scratch) HB_CUDA(cudaMallocAsync((void **)&buf, scratch * sizeof(double), s));
+  int max_levels = 0;
+  for (size_t p = 0; p < probs.size(); ++p) {
+    auto &L = levels[p];
+    L[0].A = probs[p].Y;
+    L[0].lda = probs[p].ldy;
+    for (size_t l = 1; l < L.size(); ++l) {
+      L[l].A = buf + stack_off[p][l - 1];
+      L[l].lda = L[l].rows;
+    }
+    max_levels = std::max(max_levels, (int)L.size());
+  }
+  // up-sweep
+  for (int l = 0; l < max_levels; ++l) {
+    std::vector<QrChunk> chunks;
+    for (size_t p = 0; p < probs.size(); ++p) {
+      auto &L = levels[p];
+      if (l >= (int)L.size()) continue;
+      const int w = probs[p].w;
+      for (int c = 0; c < L[l].nchunks; ++c) {
+        QrChunk q;
+        q.A = L[l].A + (long long)c * kChunk;
+        q.lda = L[l].lda;
+        q.rows = std::min(kChunk, L[l].rows - c * kChunk);
+        q.w = w;
+        if (l + 1 < (int)L.size()) {
+          q.R = L[l + 1].A + (long long)c * w;
+          q.ldr = L[l + 1].lda;
+        } else {
+          q.R = probs[p].R;
+          q.ldr = probs[p].ldr;
+        }
+        if (q.rows > 0) chunks.push_back(q);
+      }
+    }
+    launch_qr(chunks, s);
+  }
+  // down-sweep: every chunk's Q times its block of the parent's Q
+  for (int l = max_levels - 2; l >= 0; --l) {
+    std::vector<MulChunk> chunks;
+    for (size_t p = 0; p < probs.size(); ++p) {
+      auto &L = levels[p];
+      if (l + 1 >= (int)L.size()) continue;
+      const int w = probs[p].w;
+      for (int c = 0; c < L[l].nchunks; ++c) {
+        MulChunk mc;
+        mc.Q = L[l].A + (long long)c * kChunk;
+        mc.ldq = L[l].lda;
+        mc.rows = std::min(kChunk, L[l].rows - c * kChunk);
+        mc.w = w;
+        mc.M = L[l + 1].A + (long long)c * w;
+        mc.ldm = L[l + 1].lda;
+        if (mc.rows > 0) chunks.push_back(mc);
+      }
+    }
+    launch_mul(chunks, s);
+  }
+  if (buf) cudaFreeAsync(buf, s);
+}
+
+void gaussian_fill(const std::vector<RandDesc> &descs, unsigned long long seed, cudaStream_t s) {
+  if (descs.empty()) return;
+  RandDesc *d = upload(descs, s);
+  for (size_t off = 0; off < descs.size(); off += 65535) {
+    dim3 grid(64, (unsigned)std::min<size_t>(65535, descs.size() - off));
+    gaussian_kernel<<<grid, 256, 0, s>>>(d + off, seed);
+    HB_LAUNCHED();
+  }
+  cudaFreeAsync(d, s);
+}
+
+void column_norms2(const std::vector<NormDesc> &descs, cudaStream_t s) {
+  if (descs.empty()) return;
+  NormDesc *d = upload(descs, s);
+  for (size_t off = 0; off < descs.size(); off += 65535) {
+    dim3 grid(8, (unsigned)std::min<size_t>(65535, descs.size() - off));
+    colnorm_kernel<<<grid, 256, 0, s>>>(d + off);
+    HB_LAUNCHED();
+  }
+  cudaFreeAsync(d, s);
+}
+
+}  // namespace hb

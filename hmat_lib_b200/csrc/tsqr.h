@@ -1,0 +1,46 @@
+// Batched tall-skinny Householder QR (TSQR) of panels of at most 32 columns,
+// with the explicit orthonormal factor written over the input.
+#pragma once
+
+#include <vector>
+
+#include "common.h"
+
+namespace hb {
+
+constexpr int kPanel = 32;       // panel width
+constexpr int kChunk = 256;      // rows per CTA-level QR
+
+struct TsqrProb {
+  double *Y;        // m x w panel (ld ldy), overwritten by Q
+  long long ldy;
+  int m, w;         // w <= kPanel
+  double *R;        // out: w x w upper triangular (ld ldr)
+  long long ldr;
+};
+
+// Q R = Y for every problem.  Rank-deficient panels still get an orthonormal
+// Q (Householder), R then has (near-)zero diagonal entries.
+void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t stream);
+
+// Gaussian N(0, 1) entries from a counter-based hash (splitmix64 + Box-Muller):
+// entry (i, j) of matrix `id` depends only on (seed, id, i, j).
+struct RandDesc {
+  double *X;
+  long long ld;
+  int rows, cols;
+  unsigned long long id;
+};
+void gaussian_fill(const std::vector<RandDesc> &descs, unsigned long long seed,
+                   cudaStream_t stream);
+
+// Squared column norms of many matrices: out[c] = ||X[:, c]||^2.
+struct NormDesc {
+  const double *X;
+  long long ld;
+  int rows, cols;
+  double *out;
+};
+void column_norms2(const std::vector<NormDesc> &descs, cudaStream_t stream);
+
+}  // namespace hb

@@ -11,7 +11,7 @@
  * values in place).
  *
  * The functions below work on device-resident trees and device buffers
- * directly.  `stream` is a cudaStream_t (NULL: the library's own stream);
+ * directly.  `stream` is a cudaStream_t (NULL: the CUDA default stream);
  * they return an ErrorCode (error.h) and never fall back to the CPU.
  */
 #pragma once
@@ -70,6 +70,17 @@ int hodlr_b200_matmat_dev(hodlr_b200_tree t, int op, int precision, const double
 /* H1 * H2 with recompression at svd_threshold, result stays on the device. */
 int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshold,
                        hodlr_b200_tree *out, int *ierr);
+/* Kernel matrix in device memory: out_ij = k(|p_i - p_j|) + diag delta_ij,
+ * points column-major n x dim (coordinate a of point i at d_points[i + a n]);
+ * kind 0: exp(-r^2 / (2 l^2)), 1: Matern-3/2 (1 + sqrt(3) r / l) exp(-sqrt(3) r / l),
+ * 2: exp(-r / l). */
+int hodlr_b200_kernel_matrix_dev(const double *d_points, int n, int dim, int kind, double length,
+                                 double diag, double *d_out, int ld, void *stream);
+/* Device time (ms) of the two product phases accumulated since the last call
+ * while option "record_phase_times" is non-zero: out[0] projections
+ * (W = V^T X), out[1] output bands (Y = D X + sum U W), out[2] number of
+ * products.  Resets the accumulators; returns the number of values. */
+int hodlr_b200_phase_times(double *out, int capacity);
 /* Re-upload a host tree whose factor values were edited in place. */
 int hodlr_b200_sync_tree(const struct TreeHODLR *hodlr);
 

@@ -1,0 +1,84 @@
+"""Timed CPU baseline: the unmodified hmat_lib (oracle/_ref/libhmat_ref.so)
+on this machine's host cores -- TEST/BENCH INFRASTRUCTURE ONLY.
+
+    python -m oracle.cpu_baseline --n 4096 --height 5 --k 256 --steps 3
+
+Builds a Matern-3/2 kernel matrix on 2D Morton-ordered points (the family of
+the n = 32768 benchmark workload, at a size the reference can build: its
+constructor overflows `int` at n = 32768, hmat_lib src/constructors.c:676),
+times dense_to_tree_hodlr with OpenMP tasks on every core and one BLAS thread
+each, then times multiply_hodlr_dense with a threaded BLAS (the reference's
+algebra has no OpenMP).  Prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--height", type=int, default=5)
+    ap.add_argument("--k", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--threads", type=int, default=os.cpu_count())
+    ap.add_argument("--tol", type=float, default=1e-8)
+    args = ap.parse_args()
+
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    import numpy as np
+
+    from hmat_lib_b200 import workloads as W
+    from oracle import ref_lib
+
+    ref_lib.load()
+    ref_lib.set_omp_threads(args.threads)
+    ref_lib.set_blas_threads(1)
+    w = W.WORKLOADS["matern2d_n32768"]
+    pts = W.points_morton(args.n, 2, w["seed"])
+    a = W.kernel_matrix(pts, w["kind"], w["length"], w["diag"])
+    t0 = time.perf_counter()
+    tree = ref_lib.build(a, args.height, args.tol)
+    build_s = time.perf_counter() - t0
+    td = tree.data()
+    storage = td.storage()
+    x = np.asfortranarray(W.rhs(args.n, args.k, seed=1))
+    ref_lib.set_blas_threads(args.threads)
+    for _ in range(args.warmup):
+        ref_lib.multiply_dense(tree, x, "N")
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref_lib.multiply_dense(tree, x, "N")
+        times.append(time.perf_counter() - t0)
+    step = float(np.median(times))
+    nbytes = 8.0 * storage + 16.0 * args.n * args.k
+    flops = 2.0 * args.k * storage
+    print(json.dumps(dict(
+        n=args.n, height=args.height, k=args.k, tol=args.tol, threads=args.threads,
+        build_s=build_s, matmat_s=step, matmat_gbs=nbytes / step / 1e9,
+        matmat_gflops=flops / step / 1e9, storage=int(storage),
+        max_rank=int(max(td.ranks().values())),
+        cpu=_cpu_model())))
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+if __name__ == "__main__":
+    main()

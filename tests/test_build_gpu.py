@@ -123,3 +123,41 @@ def test_jacobi_sweep_cap_reports_svd_failure(lib):
         assert e.value.code == abi.SVD_FAILURE
     finally:
         lib.hodlr_b200_set_option(b"jacobi_max_sweeps", 60.0)
+
+
+def test_sketched_path_known_answers(lib):
+    """Force the randomized path for every block wider than 8 columns and
+    re-run hmat_lib's dense_to_tree known answers."""
+    lib.hodlr_b200_set_option(b"exact_max", 8.0)
+    try:
+        for c in K.known_answers()["dense_to_tree"]:
+            a = K.dense_case_matrix(c)
+            t = Tree.from_dense(a, c["height"], 1e-8, c["ms"])
+            td = t.data()
+            assert np.abs(td.to_dense() - a).max() <= K.DELTA, c["name"]
+            for (d, j, cc), (u, v) in td.blocks.items():
+                want = c["root_rank"] if d == 0 else c["other_rank"]
+                if want > 0:
+                    assert u.shape[1] == want, (c["name"], d, j, cc)
+            t.free()
+    finally:
+        lib.hodlr_b200_set_option(b"exact_max", 128.0)
+
+
+@pytest.mark.parametrize("n,h", [(2048, 4), (4096, 5)])
+def test_sketched_build_2d_matern(n, h):
+    """The benchmark's kernel family (2D Matern-3/2, l = 0.1, tol 1e-8) at
+    sizes the CPU oracle handles: ranks within one of the oracle's dgesdd
+    ranks, reconstruction and products within the truncation tolerance."""
+    pts = W.points_morton(n, 2, seed=1)
+    a = W.kernel_matrix(pts, "matern32", 0.1, 1e-2)
+    t = Tree.from_dense(a, h, 1e-8)
+    td = t.data()
+    ot = O.dense_to_tree(a, h, 1e-8)
+    for key, r in ot.ranks().items():
+        assert abs(td.ranks()[key] - r) <= 1, (key, td.ranks()[key], r)
+    assert O.rel_fro(td.to_dense(), a) < 1e-8
+    x = np.asfortranarray(np.random.default_rng(3).standard_normal((n, 16)))
+    assert O.rel_fro(t.matmat(x), a @ x) < 1e-8
+    assert O.rel_fro(t.matmat(x), O.multiply_dense(ot, x)) < 1e-8
+    t.free()
