@@ -155,7 +155,9 @@ int dense_to_tree_hodlr(TreeHODLR *hodlr, const int m, const int *ms, double *ma
     register_device_tree(hodlr, dt);
     if (status != SUCCESS) {
       *ierr = status;
-      set_last_error("Jacobi SVD did not converge within the sweep limit");
+      const BuildStats &st = last_build_stats();
+      set_last_error(st.cap_hit ? "a block's rank reached the sketch cap (option sketch_cap)"
+                                : "Jacobi SVD did not converge within the sweep limit");
       return 1;
     }
     return 0;
@@ -457,6 +459,18 @@ int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshol
 }
 
 int hodlr_b200_phase_times(double *out, int capacity) { return phase_times(out, capacity); }
+
+int hodlr_b200_build_stats(double *out, int capacity) {
+  const BuildStats &st = last_build_stats();
+  const double v[] = {(double)st.exact_blocks,     (double)st.sketched_blocks,
+                      (double)st.sketch_rounds,    st.seconds,
+                      (double)st.cap_hit,          (double)st.max_sweeps_exact,
+                      (double)st.max_sweeps_sketch, (double)st.failed_exact,
+                      (double)st.failed_sketch,    (double)st.max_sketch};
+  const int n = (int)(sizeof(v) / sizeof(v[0]));
+  for (int i = 0; i < n && i < capacity && out; ++i) out[i] = v[i];
+  return n;
+}
 
 int hodlr_b200_sync_tree(const TreeHODLR *hodlr) {
   try {

@@ -52,7 +52,11 @@ struct SketchBlock {
   int last_pw = 0;
 };
 
+thread_local BuildStats g_last_stats;
+
 }  // namespace
+
+const BuildStats &last_build_stats() { return g_last_stats; }
 
 std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double *d_A,
                                              long long lda, double tol, cudaStream_t stream,
@@ -115,7 +119,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     S.om = take((long long)B.n * w_max);
     S.t = take((long long)S.cap * w_max);
     S.c = take((long long)S.cap * kPanel);
-    S.rn = take((long long)kPanel * kPanel + w_max);
+    S.rn = take((long long)kPanel * kPanel + kPanel + w_max);
     sk.push_back(S);
   }
   double *work = dev_alloc(scratch, stream);
@@ -125,11 +129,14 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   for (int i = 2; i < kGemmBases; ++i) bases.p[i] = work;
   if (!sk.empty()) HB_CUDA(cudaMemsetAsync(work, 0, scratch * sizeof(double), stream));
 
-  int *d_int = nullptr;   // ranks of exact blocks, ranks of sketched blocks, status
+  // ranks of exact blocks, ranks of sketched blocks, status, then the sweeps
+  // used by every Jacobi problem in the same order
+  int *d_int = nullptr;
   const int n_int = (int)exact.size() + (int)sk.size() + 1;
-  HB_CUDA(cudaMallocAsync((void **)&d_int, sizeof(int) * n_int, stream));
-  HB_CUDA(cudaMemsetAsync(d_int, 0, sizeof(int) * n_int, stream));
+  HB_CUDA(cudaMallocAsync((void **)&d_int, sizeof(int) * 2 * n_int, stream));
+  HB_CUDA(cudaMemsetAsync(d_int, 0, sizeof(int) * 2 * n_int, stream));
   int *d_status = d_int + n_int - 1;
+  int *d_sweeps = d_int + n_int;
   JacobiParams prm;
   prm.tol = tol;
   prm.trunc = Truncation::Relative;
@@ -155,6 +162,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     jp.ldv = B.n;
     jp.sigma = work + eslots[p].sig;
     jp.rank = d_int + p;
+    jp.sweeps = d_sweeps + p;
     eprobs.push_back(jp);
   }
   JacobiProb *d_eprobs = nullptr;
@@ -201,6 +209,14 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
         g1.seg(pr, kA, S.a_off, lda, 0, kWork, S.om, S.n, 0, S.n);
       }
       gemm_f64_run(g1, bases, TileShape::M128N64, stream);
+      // ||A om_c||^2: the scale against which a projected column counts as noise
+      std::vector<NormDesc> nd;
+      for (int i : act) {
+        const SketchBlock &S = sk[i];
+        nd.push_back(NormDesc{work + S.q + (long long)S.ell * S.m, S.m, S.m, wb[i],
+                              work + S.rn + kPanel * kPanel + kPanel});
+      }
+      column_norms2(nd, stream);
       GemmBatch g2;
       for (int i : act) {
         const SketchBlock &S = sk[i];
@@ -279,6 +295,15 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
           if (left) sk[i].last_pw = pw;
         }
         tsqr_batched(tp, stream);
+        if (left) {
+          std::vector<CleanDesc> cd;
+          for (size_t a = 0; a < pa.size(); ++a) {
+            const SketchBlock &S = sk[pa[a]];
+            cd.push_back(CleanDesc{tp[a].Y, tp[a].ldy, tp[a].m, tp[a].w, tp[a].R, tp[a].ldr,
+                                   work + S.rn + kPanel * kPanel + kPanel + q * kPanel});
+          }
+          panel_clean(cd, option("sketch_clean_rel", 1e-13), stream);
+        }
       }
     };
     orthonormalise(true);
@@ -385,6 +410,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
       jp.sigma = jwork + o;
       o += align_up(L);
       jp.rank = d_int + exact.size() + i;
+      jp.sweeps = d_sweeps + exact.size() + i;
       sprobs.push_back(jp);
     }
   }
@@ -393,8 +419,8 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     d_sprobs = upload_vec(sprobs, stream);
     jacobi_svd_batched(d_sprobs, (int)sprobs.size(), prm, d_status, max_l, stream);
   }
-  std::vector<int> ints(n_int, 0);
-  HB_CUDA(cudaMemcpyAsync(ints.data(), d_int, sizeof(int) * n_int, cudaMemcpyDeviceToHost,
+  std::vector<int> ints(2 * n_int, 0);
+  HB_CUDA(cudaMemcpyAsync(ints.data(), d_int, sizeof(int) * 2 * n_int, cudaMemcpyDeviceToHost,
                           stream));
   HB_CUDA(cudaStreamSynchronize(stream));
   *svd_status = ints[n_int - 1];
@@ -452,13 +478,26 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     *svd_status = SVD_FAILURE;
     set_last_error("a block's rank reached the sketch cap (option sketch_cap)");
   }
-  if (stats) {
-    stats->exact_blocks = (int)exact.size();
-    stats->sketched_blocks = (int)sk.size();
-    stats->sketch_rounds = rounds;
-    stats->seconds =
-        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  BuildStats st;
+  st.exact_blocks = (int)exact.size();
+  st.sketched_blocks = (int)sk.size();
+  st.sketch_rounds = rounds;
+  st.cap_hit = cap_hit ? 1 : 0;
+  const int maxsw = prm.max_sweeps;
+  for (size_t p = 0; p < exact.size(); ++p) {
+    const int sw = ints[n_int + p];
+    st.max_sweeps_exact = std::max(st.max_sweeps_exact, sw);
+    st.failed_exact += sw > maxsw;
   }
+  for (size_t i = 0; i < sk.size(); ++i) {
+    const int sw = ints[n_int + exact.size() + i];
+    st.max_sweeps_sketch = std::max(st.max_sweeps_sketch, sw);
+    st.failed_sketch += sw > maxsw;
+    st.max_sketch = std::max(st.max_sketch, sk[i].ell);
+  }
+  st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  g_last_stats = st;
+  if (stats) *stats = st;
   return dt;
 }
 

@@ -10,7 +10,14 @@ struct BuildStats {
   int sketched_blocks = 0;     // blocks compressed by the randomized path
   int sketch_rounds = 0;       // adaptive growth rounds of the randomized path
   double seconds = 0.0;
+  int cap_hit = 0;             // a sketch reached its column cap
+  int max_sweeps_exact = 0, max_sweeps_sketch = 0;
+  int failed_exact = 0, failed_sketch = 0;
+  int max_sketch = 0;          // largest sketch (columns)
 };
+
+// Statistics of the most recent build on the calling thread.
+const BuildStats &last_build_stats();
 
 // Compresses every off-diagonal block of the n x n matrix d_A (ld lda, device)
 // following the block sizes of `g` (ranks ignored) with hmat_lib's relative

@@ -7,6 +7,7 @@
 // memory as double2.  FP64 has no tcgen05 path; this is the FP64 roofline
 // kernel (B200: 64 DFMA / clock / SM).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "gemm_f64.h"
@@ -258,10 +259,13 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
     GemmProb &P = probs[p];
     if (P.M <= 0 || P.N <= 0) continue;
     const int mt = (P.M + BM - 1) / BM, nt = (P.N + BN - 1) / BN;
+    // Split K so that no tile carries much more than an even share of the
+    // batch's work (the longest tile bounds the launch), and to fill the GPU.
     long long split = 1;
-    if (allow_split && base_tiles < target && ktot[p] > 4 * 256) {
-      const double share = (double)mt * nt * (double)ktot[p] / work;
-      split = (long long)(share * (double)target / (double)(mt * nt) + 0.5);
+    if (allow_split && ktot[p] > 2 * 256) {
+      const double per_tile = work / (double)target;          // ideal work per tile
+      const double mine = (double)std::max<long long>(ktot[p], 1);
+      split = (long long)std::ceil(mine / std::max(per_tile, 512.0));
       split = std::max<long long>(1, std::min<long long>(split, ktot[p] / 256));
     }
     long long chunk = (ktot[p] + split - 1) / split;

@@ -53,6 +53,9 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
     W[e] = ((e % C) == (e / C)) ? 1.0 : 0.0;
   __syncthreads();
 
+  // a computed dot product of length R carries ~sqrt(R) eps relative noise:
+  // below that no rotation can make progress
+  const double conv = fmax(prm.conv_tol, 4.0 * sqrt((double)R) * 2.220446049250313e-16);
   const int players = C + (C & 1);
   int sweep = 0;
   bool converged = (C == 1);
@@ -84,9 +87,13 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
         if (ga == 0.0 || al <= 0.0 || be <= 0.0) continue;
         const double rel = fabs(ga) / (sqrt(al) * sqrt(be));
         off = fmax(off, rel);
-        if (rel <= prm.conv_tol) continue;
+        if (rel <= conv) continue;
         const double zeta = (be - al) / (2.0 * ga);
-        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        // tan of the rotation angle; for |zeta| beyond 1e100 zeta^2 would
+        // overflow and the exact value is 1 / (2 zeta) to double precision
+        const double t = fabs(zeta) > 1e100
+                             ? 0.5 / zeta
+                             : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
         const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
         for (int i = lane; i < R; i += 32) {
           const double x = gp[i], y = gq[i];
@@ -109,10 +116,11 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
     __syncthreads();
     double mx = 0.0;
     for (int w = 0; w < nwarps; ++w) mx = fmax(mx, s_off[w]);
-    converged = mx <= prm.conv_tol;
+    converged = mx <= conv;
     __syncthreads();
   }
   if (!converged && tid == 0) atomicExch(status, (int)SVD_FAILURE);
+  if (tid == 0 && P.sweeps) *P.sweeps = converged ? sweep : prm.max_sweeps + 1;
 
   // singular values = column norms of G
   for (int j = warp; j < C; j += nwarps) {

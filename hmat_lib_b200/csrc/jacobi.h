@@ -22,6 +22,7 @@ struct JacobiProb {
   long long ldv;
   double *sigma;    // out: C singular values, descending
   int *rank;        // out: truncation rank (>= 1 unless the block is empty)
+  int *sweeps;      // out (optional): sweeps used; max_sweeps + 1 if not converged
 };
 
 enum class Truncation : int {

@@ -231,7 +231,30 @@ void launch_mul(const std::vector<MulChunk> &chunks, cudaStream_t s) {
   cudaFreeAsync(d, s);
 }
 
+__global__ void panel_clean_kernel(const CleanDesc *__restrict__ descs, double rel) {
+  const CleanDesc D = descs[blockIdx.y];
+  double scale2 = 0.0;
+  for (int c = 0; c < D.w; ++c) scale2 = fmax(scale2, D.prenorm2[c]);
+  const double thr = rel * sqrt(scale2);
+  for (int c = 0; c < D.w; ++c) {
+    if (fabs(D.R[c + (long long)c * D.ldr]) > thr) continue;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.rows; i += gridDim.x * blockDim.x)
+      D.Q[i + (long long)c * D.ldq] = 0.0;
+  }
+}
+
 }  // namespace
+
+void panel_clean(const std::vector<CleanDesc> &descs, double rel, cudaStream_t s) {
+  if (descs.empty()) return;
+  CleanDesc *d = upload(descs, s);
+  for (size_t off = 0; off < descs.size(); off += 65535) {
+    dim3 grid(8, (unsigned)std::min<size_t>(65535, descs.size() - off));
+    panel_clean_kernel<<<grid, 256, 0, s>>>(d + off, rel);
+    HB_LAUNCHED();
+  }
+  cudaFreeAsync(d, s);
+}
 
 void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t s) {
   if (probs.empty()) return;

@@ -23,6 +23,22 @@ struct TsqrProb {
 // Q (Householder), R then has (near-)zero diagonal entries.
 void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t stream);
 
+// Zeroes the columns of a freshly orthonormalised sketch panel whose R
+// diagonal is at rounding level, |R_jj| <= rel * max_c ||Y_c||, where ||Y_c||
+// are the panel's column norms before projection.  A Gaussian sketch of a
+// residual of rank r < w has its r independent columns first, so these are
+// the trailing columns that carry no new direction; left in place they would
+// not be orthogonal to the existing basis.
+struct CleanDesc {
+  double *Q;
+  long long ldq;
+  int rows, w;
+  const double *R;
+  long long ldr;
+  const double *prenorm2;
+};
+void panel_clean(const std::vector<CleanDesc> &descs, double rel, cudaStream_t stream);
+
 // Gaussian N(0, 1) entries from a counter-based hash (splitmix64 + Box-Muller):
 // entry (i, j) of matrix `id` depends only on (seed, id, i, j).
 struct RandDesc {

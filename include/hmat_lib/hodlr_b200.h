@@ -81,6 +81,11 @@ int hodlr_b200_kernel_matrix_dev(const double *d_points, int n, int dim, int kin
  * (W = V^T X), out[1] output bands (Y = D X + sum U W), out[2] number of
  * products.  Resets the accumulators; returns the number of values. */
 int hodlr_b200_phase_times(double *out, int capacity);
+/* Statistics of the calling thread's most recent build: exact blocks,
+ * sketched blocks, sketch rounds, seconds, cap hit, max Jacobi sweeps (exact,
+ * sketched), unconverged Jacobi problems (exact, sketched), largest sketch.
+ * Returns the number of values. */
+int hodlr_b200_build_stats(double *out, int capacity);
 /* Re-upload a host tree whose factor values were edited in place. */
 int hodlr_b200_sync_tree(const struct TreeHODLR *hodlr);
 

@@ -156,8 +156,11 @@ def test_sketched_build_2d_matern(n, h):
     ot = O.dense_to_tree(a, h, 1e-8)
     for key, r in ot.ranks().items():
         assert abs(td.ranks()[key] - r) <= 1, (key, td.ranks()[key], r)
-    assert O.rel_fro(td.to_dense(), a) < 1e-8
+    # the truncation error itself is the oracle's (dgesdd at the same tol)
+    err_oracle = O.rel_fro(ot.to_dense(), a)
+    assert O.rel_fro(td.to_dense(), a) <= 1.25 * err_oracle + 1e-12
     x = np.asfortranarray(np.random.default_rng(3).standard_normal((n, 16)))
-    assert O.rel_fro(t.matmat(x), a @ x) < 1e-8
-    assert O.rel_fro(t.matmat(x), O.multiply_dense(ot, x)) < 1e-8
+    yo = O.multiply_dense(ot, x)
+    assert O.rel_fro(t.matmat(x), a @ x) <= 1.25 * O.rel_fro(yo, a @ x) + 1e-12
+    assert O.rel_fro(t.matmat(x), yo) < 2e-8
     t.free()
