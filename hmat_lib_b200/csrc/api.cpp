@@ -19,10 +19,6 @@
 
 using namespace hb;
 
-struct hodlr_b200_tree_s {
-  std::shared_ptr<DeviceTree> p;
-};
-
 namespace {
 
 int fail(int *ierr, const Error &e) {

@@ -9,6 +9,7 @@ namespace hb {
 
 namespace {
 thread_local std::string g_last_error;
+thread_local const char *g_static_error = nullptr;
 std::atomic<long long> g_launches{0};
 std::mutex g_opt_mutex;
 std::map<std::string, double> &opts() {
@@ -17,8 +18,12 @@ std::map<std::string, double> &opts() {
 }
 }  // namespace
 
-void set_last_error(const std::string &msg) { g_last_error = msg; }
-const char *last_error() { return g_last_error.c_str(); }
+void set_last_error(const std::string &msg) {
+  g_static_error = nullptr;
+  g_last_error = msg;
+}
+void set_last_error_static(const char *msg) { g_static_error = msg; }
+const char *last_error() { return g_static_error ? g_static_error : g_last_error.c_str(); }
 
 void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 long long launches() { return g_launches.load(); }

@@ -20,6 +20,8 @@ struct Error {
 };
 
 void set_last_error(const std::string &msg);
+// Records a message that is a string literal, without allocating.
+void set_last_error_static(const char *msg);
 const char *last_error();
 
 #define HB_CUDA(call)                                                        \

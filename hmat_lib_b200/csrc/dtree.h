@@ -62,3 +62,8 @@ double *dev_alloc(size_t elems, cudaStream_t stream);
 void dev_free(void *p, cudaStream_t stream);
 
 }  // namespace hb
+
+// The opaque handle of include/hmat_lib/hodlr_b200.h.
+struct hodlr_b200_tree_s {
+  std::shared_ptr<hb::DeviceTree> p;
+};

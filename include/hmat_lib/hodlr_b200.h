@@ -86,6 +86,21 @@ int hodlr_b200_phase_times(double *out, int capacity);
  * sketched), unconverged Jacobi problems (exact, sketched), largest sketch.
  * Returns the number of values. */
 int hodlr_b200_build_stats(double *out, int capacity);
+/* y = H x on device buffers, allocating nothing (no counterpart in hmat_lib).
+ * For callers that cannot allocate device memory while they run: an
+ * iterative solver whose memory pool already holds nearly all of HBM, or
+ * latency-critical code that cannot afford cudaMalloc's implicit device
+ * synchronisation.  The per-block projections V_b^T x, the product's only
+ * scratch, live in a fixed 528 KiB array of device memory inside the library
+ * (held on every GPU that loads it, until exit) instead of a per-call
+ * allocation.  Limits: the ranks of the tree sum to at most 65536 and it has
+ * at most 4096 off-diagonal blocks; larger trees return INPUT_ERROR with a
+ * message.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (unordered streams) race;
+ * order them on one stream.  Returns an ErrorCode. */
+int hodlr_b200_matvec_noalloc_dev(hodlr_b200_tree t, const double *d_x, double *d_y,
+                                  void *stream);
 /* Re-upload a host tree whose factor values were edited in place. */
 int hodlr_b200_sync_tree(const struct TreeHODLR *hodlr);
 
