@@ -304,20 +304,27 @@ def main():
             pg.destroy_process_group()
         return
 
-    # ---- roofline of the dominant kernel (phase 2: output bands) --------------------
-    p1_ms, p2_ms, cnt = pt[0] / max(pt[2], 1), pt[1] / max(pt[2], 1), pt[2]
-    # phase 2 streams every leaf and U factor once and writes Y: its algorithmic
-    # work is 2 k (sum m_leaf^2 + sum s m) flops; phase 1 is 2 k sum s n
-    peak = fp64_peak_tflops(torch, dev)
-    dom = "phase2" if p2_ms >= p1_ms else "phase1"
+    # ---- roofline of the dominant kernel ---------------------------------------------
+    # Per-phase algorithmic work from the block ranks (halving geometry: every
+    # block at depth d is n / 2^(d+1) square).  Phase 1 reads V and X
+    # (2 k sum s_b n_b flops); phase 2 reads the leaves, U and X and writes Y
+    # (2 k (sum m_leaf^2 + sum s_b m_b) flops).
+    sn = sum(int(ranks[b]) * (n >> ((b // 2 + 1).bit_length())) for b in range(len(ranks)))
     n_leaf = 1 << h
-    leaf = n // n_leaf
-    leaves_el = n_leaf * leaf * leaf
-    lowrank_el = storage - leaves_el
-    p2_flops = 2.0 * k * (leaves_el + lowrank_el / 2.0)
-    p1_flops = 2.0 * k * (lowrank_el / 2.0)
-    dom_flops, dom_ms = (p2_flops, p2_ms) if dom == "phase2" else (p1_flops, p1_ms)
-    achieved = dom_flops / (dom_ms * 1e-3) / 1e12
+    leaves_el = n_leaf * (n // n_leaf) ** 2
+    phase = {
+        "phase1": dict(ms=pt[0] / max(pt[2], 1), flops=2.0 * k * sn,
+                       bytes=8.0 * sn + 8.0 * n * k),
+        "phase2": dict(ms=pt[1] / max(pt[2], 1), flops=2.0 * k * (leaves_el + sn),
+                       bytes=8.0 * (leaves_el + sn) + 16.0 * n * k),
+    }
+    # DRAM traffic / algorithmic bytes of each phase, measured by ncu on the
+    # n = 16384 instance of this workload (profiles/matmat_fp64_gemm_n16384_k256.md);
+    # traffic grows with the factors, so it is scaled by the algorithmic bytes.
+    traffic_ratio = {"phase1": 1.31, "phase2": 1.14}
+    dom = max(phase, key=lambda p: phase[p]["ms"])
+    peak = fp64_peak_tflops(torch, dev)
+    achieved = phase[dom]["flops"] / (phase[dom]["ms"] * 1e-3) / 1e12
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         res = run_cpu_baseline(args.cpu_n, k)
@@ -345,10 +352,15 @@ def main():
                  "ranks_by_depth": [int(max(ranks[2 * ((1 << d) - 1):2 * ((1 << (d + 1)) - 1)]))
                                     for d in range(h)]},
         "gflops": flops_step / (ms_step * 1e-3) / 1e9,
-        "roofline": {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+        "roofline": {"bound": "fp64", "kernel": f"gemm_f64_kernel ({dom})", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": traffic_ratio[dom] * phase[dom]["bytes"],
+                     "traffic_note": "ncu dram bytes/algorithmic bytes at n=16384, scaled",
+                     "algorithmic_bytes": phase[dom]["bytes"],
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-                     "phase_ms": {"phase1": p1_ms, "phase2": p2_ms}},
+                     "phase_ms": {p: phase[p]["ms"] for p in phase},
+                     "phase_tflops": {p: phase[p]["flops"] / (phase[p]["ms"] * 1e-3) / 1e12
+                                      for p in phase}},
         "clocks": clk.summary(),
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": int(8 * n * k),
                 "d2h_bytes_per_step": int(8 * n * k), "ms_per_step": e2e_s * 1e3},

@@ -25,7 +25,7 @@ struct DeviceTree {
   LeafDesc *d_leaves = nullptr;
   BlockDesc *d_blocks = nullptr;
   uint64_t fingerprint = 0;         // of the host tree this mirrors (0: none)
-  std::map<std::tuple<int, int, long long, long long, int>, std::unique_ptr<ProductPlan>> plans;
+  std::map<std::tuple<int, int, long long, long long, int, int>, std::unique_ptr<ProductPlan>> plans;
   std::mutex plan_mutex;
 
   DeviceTree() = default;

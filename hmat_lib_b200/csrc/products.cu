@@ -40,9 +40,9 @@ static int covering_block(int h, int i, int d, bool row_side) {
 }
 
 ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, int min_depth) {
   std::lock_guard<std::mutex> lk(t.plan_mutex);
-  auto key = std::make_tuple((int)op, k, ldx, ldy, (int)Precision::FP64);
+  auto key = std::make_tuple((int)op, k, ldx, ldy, (int)Precision::FP64, min_depth);
   auto it = t.plans.find(key);
   if (it != t.plans.end()) return *it->second;
 
@@ -66,7 +66,7 @@ ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long l
   GemmBatch p1;
   for (size_t bi = 0; bi < g.blocks.size(); ++bi) {
     const BlockDesc &b = g.blocks[bi];
-    if (b.s == 0) continue;
+    if (b.s == 0 || b.depth < min_depth) continue;
     if (op == ProdOp::N) {          // W_b (s x k) = V_b^T X[c0 : c0 + n]
       int p = p1.add(kW, w_off[bi], b.s, b.s, k);
       p1.seg(p, kArena, b.v_off, b.n, 1, kX, b.c0, ldx, 0, b.n);
@@ -86,7 +86,7 @@ ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long l
     if (op == ProdOp::N || op == ProdOp::T) {
       int p = p2.add(kY, L.r0, ldy, L.m, k);
       p2.seg(p, kArena, L.off, L.m, op == ProdOp::T ? 1 : 0, kX, L.r0, ldx, 0, L.m);
-      for (int d = h - 1; d >= 0; --d) {
+      for (int d = h - 1; d >= min_depth; --d) {
         const int bi = covering_block(h, i, d, op == ProdOp::N);
         const BlockDesc &b = g.blocks[bi];
         if (b.s == 0) continue;
@@ -98,7 +98,7 @@ ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long l
     } else {
       int p = p2.add(kY, (long long)L.r0 * ldy, ldy, k, L.m);
       p2.seg(p, kX, (long long)L.r0 * ldx, ldx, 0, kArena, L.off, L.m, 0, L.m);
-      for (int d = h - 1; d >= 0; --d) {
+      for (int d = h - 1; d >= min_depth; --d) {
         const int bi = covering_block(h, i, d, false);
         const BlockDesc &b = g.blocks[bi];
         if (b.s == 0) continue;
@@ -155,9 +155,9 @@ int phase_times(double *out, int cap) {
 }
 
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
-                 long long ldy, cudaStream_t stream) {
+                 long long ldy, cudaStream_t stream, int min_depth) {
   if (k <= 0 || t.g.n == 0) return;
-  ProductPlan &plan = product_plan(t, op, k, ldx, ldy, stream);
+  ProductPlan &plan = product_plan(t, op, k, ldx, ldy, stream, min_depth);
   GemmBases bases{};
   bases.p[kArena] = t.arena;
   bases.p[kX] = const_cast<double *>(X);

@@ -42,8 +42,11 @@ struct ProductWork {
 ProductWork product_work(const DeviceTree &t, int k);
 
 // Runs Y = op(H, X) with X, Y device pointers (column-major, ld given).
+// With min_depth > 0 only the diagonal leaves and the off-diagonal blocks of
+// depth >= min_depth take part: the block-diagonal product of all subtrees
+// rooted at that depth (used by HODLR x HODLR).
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
-                 long long ldy, cudaStream_t stream);
+                 long long ldy, cudaStream_t stream, int min_depth = 0);
 
 // Accumulated per-phase device times (ms) of products run with option
 // "record_phase_times" set: out[0] phase 1, out[1] phase 2, out[2] count.
@@ -52,6 +55,6 @@ int phase_times(double *out, int cap);
 
 // Builds (and caches on the tree) the plan for this shape without running it.
 ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,
-                          cudaStream_t stream);
+                          cudaStream_t stream, int min_depth = 0);
 
 }  // namespace hb
