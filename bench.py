@@ -131,6 +131,31 @@ def fp64_peak_tflops(torch, dev):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
+def int8_peak_tops(torch, dev):
+    """int8 tensor throughput of cuBLASLt (torch._int_mm, 8192^3) on this GPU,
+    the denominator of the mixed path's roofline; falls back to twice the
+    measured BF16 figure when the int8 GEMM is unavailable."""
+    try:
+        a = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device=dev)
+        b = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device=dev)
+        bt = b.t()
+        for _ in range(2):
+            torch._int_mm(a, bt)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = float("inf")
+        for _ in range(5):
+            e0.record()
+            torch._int_mm(a, bt)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12, "cuBLASLt int8 GEMM 8192^3 measured in this run"
+    except Exception:
+        bf16 = measured_peaks().get("bf16_tflops", 1590.0)
+        return 2.0 * bf16, "2 x measured BF16 dense peak (int8 GEMM unavailable)"
+
+
 def run_cpu_baseline(n: int, k: int):
     cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--n", str(n),
            "--height", str(max(1, (n // 128).bit_length() - 1)), "--k", str(k), "--steps", "3"]
@@ -242,41 +267,58 @@ def main():
     del a, a_mat, y_dense
     torch.cuda.empty_cache()
 
+    # ---- mixed-precision accuracy (same X) ---------------------------------------------
+    y_mx = torch.zeros(k, n, dtype=torch.float64, device=dev)
+    tree.matmat(x.data_ptr(), k, n, y_mx.data_ptr(), n, stream=sh, precision=1)
+    stream.synchronize()
+    assert lib.hodlr_b200_check(tree.h, C.c_void_p(sh)) == 0, lib.hodlr_b200_last_error()
+    rel_err_mixed_vs_fp64 = (torch.linalg.norm(y_mx - y) / torch.linalg.norm(y)).item()
+    del y_mx
+
     # ---- timed device-resident products -------------------------------------------
     storage = info["storage"]
     bytes_step = 8.0 * storage + 16.0 * n * k
     flops_step = 2.0 * k * storage
-    for _ in range(args.warmup):
-        tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
-    stream.synchronize()
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
-    lib.hodlr_b200_set_option(b"record_phase_times", 1.0)
-    lib.hodlr_b200_phase_times(None, 0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = lib.hodlr_b200_kernel_launches()
-    with ClockSampler(local) as clk:
-        torch.cuda.nvtx.range_push("matmat")     # lets ncu select the timed launches
-        e0.record(stream)
-        for _ in range(args.steps):
-            tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
-        e1.record(stream)
+
+    def timed(precision, steps, tag):
+        for _ in range(args.warmup):
+            tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh, precision=precision)
         stream.synchronize()
-        torch.cuda.nvtx.range_pop()
-    launches = lib.hodlr_b200_kernel_launches() - launches0
-    lib.hodlr_b200_set_option(b"record_phase_times", 0.0)
-    pt = (C.c_double * 3)()
-    lib.hodlr_b200_phase_times(pt, 3)
-    ms_total = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([ms_total], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_total = t.item()
-        pg.barrier()
-    torch.cuda.synchronize()
-    ms_step = ms_total / args.steps
-    value = bytes_step * world / (ms_step * 1e-3) / 1e9
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        lib.hodlr_b200_set_option(b"record_phase_times", 1.0)
+        lib.hodlr_b200_phase_times(None, 0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = lib.hodlr_b200_kernel_launches()
+        with ClockSampler(local) as clk:
+            torch.cuda.nvtx.range_push(tag)     # lets ncu select the timed launches
+            e0.record(stream)
+            for _ in range(steps):
+                tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh, precision=precision)
+            e1.record(stream)
+            stream.synchronize()
+            torch.cuda.nvtx.range_pop()
+        launches = lib.hodlr_b200_kernel_launches() - launches0
+        lib.hodlr_b200_set_option(b"record_phase_times", 0.0)
+        pt = (C.c_double * 3)()
+        lib.hodlr_b200_phase_times(pt, 3)
+        ms_total = e0.elapsed_time(e1)
+        if pg:
+            t = torch.tensor([ms_total], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms_total = t.item()
+            pg.barrier()
+        torch.cuda.synchronize()
+        return dict(ms=ms_total / steps, launches=int(launches), clocks=clk.summary(),
+                    p1=pt[0] / max(pt[2], 1), p2=pt[1] / max(pt[2], 1))
+
+    r64 = timed(0, max(20, args.steps // 4), "matmat")
+    rmx = timed(1, args.steps, "matmat_mixed")
+    assert lib.hodlr_b200_check(tree.h, C.c_void_p(sh)) == 0, lib.hodlr_b200_last_error()
+    value = bytes_step * world / (rmx["ms"] * 1e-3) / 1e9
+    value_fp64 = bytes_step * world / (r64["ms"] * 1e-3) / 1e9
+    ms_step = rmx["ms"]
 
     # ---- e2e through the C-ABI with host buffers ------------------------------------
     host_tree = tree.to_host()
@@ -285,18 +327,26 @@ def main():
     ierr = C.c_int(0)
     xp = C.cast(C.c_void_p(xh.data_ptr()), abi.DP)
     yp = C.cast(C.c_void_p(yh.data_ptr()), abi.DP)
-    for _ in range(max(1, args.warmup)):
-        lib.multiply_hodlr_dense(host_tree.tp, xp, k, n, yp, n, C.byref(ierr))
-    assert ierr.value == 0
-    e2e_steps = max(3, args.steps // 2)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        lib.multiply_hodlr_dense(host_tree.tp, xp, k, n, yp, n, C.byref(ierr))
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if pg:
-        t = torch.tensor([e2e_s], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = t.item()
+
+    def e2e_time(precision):
+        lib.hodlr_b200_set_option(b"matmat_precision", float(precision))
+        for _ in range(max(1, args.warmup)):
+            lib.multiply_hodlr_dense(host_tree.tp, xp, k, n, yp, n, C.byref(ierr))
+        assert ierr.value == 0
+        steps = max(5, args.steps // 10)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            lib.multiply_hodlr_dense(host_tree.tp, xp, k, n, yp, n, C.byref(ierr))
+        sec = (time.perf_counter() - t0) / steps
+        lib.hodlr_b200_set_option(b"matmat_precision", 0.0)
+        if pg:
+            t = torch.tensor([sec], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            sec = t.item()
+        return sec
+
+    e2e_s_fp64 = e2e_time(0)
+    e2e_s = e2e_time(1)
     e2e = bytes_step * world / e2e_s / 1e9
 
     if rank != 0:
@@ -308,23 +358,25 @@ def main():
     # Per-phase algorithmic work from the block ranks (halving geometry: every
     # block at depth d is n / 2^(d+1) square).  Phase 1 reads V and X
     # (2 k sum s_b n_b flops); phase 2 reads the leaves, U and X and writes Y
-    # (2 k (sum m_leaf^2 + sum s_b m_b) flops).
+    # (2 k (sum m_leaf^2 + sum s_b m_b) flops).  The mixed path runs every such
+    # multiply-add as S(S+1)/2 = 21 int8 slice products on the tensor cores.
     sn = sum(int(ranks[b]) * (n >> ((b // 2 + 1).bit_length())) for b in range(len(ranks)))
     n_leaf = 1 << h
     leaves_el = n_leaf * (n // n_leaf) ** 2
-    phase = {
-        "phase1": dict(ms=pt[0] / max(pt[2], 1), flops=2.0 * k * sn,
-                       bytes=8.0 * sn + 8.0 * n * k),
-        "phase2": dict(ms=pt[1] / max(pt[2], 1), flops=2.0 * k * (leaves_el + sn),
-                       bytes=8.0 * (leaves_el + sn) + 16.0 * n * k),
-    }
-    # DRAM traffic / algorithmic bytes of each phase, measured by ncu on the
-    # n = 16384 instance of this workload (profiles/matmat_fp64_gemm_n16384_k256.md);
-    # traffic grows with the factors, so it is scaled by the algorithmic bytes.
-    traffic_ratio = {"phase1": 1.31, "phase2": 1.14}
-    dom = max(phase, key=lambda p: phase[p]["ms"])
-    peak = fp64_peak_tflops(torch, dev)
-    achieved = phase[dom]["flops"] / (phase[dom]["ms"] * 1e-3) / 1e12
+    el = {"phase1": sn, "phase2": leaves_el + sn}
+    slice_products = 21
+    peak_i8, peak_src = int8_peak_tops(torch, dev)
+    peak64 = fp64_peak_tflops(torch, dev)
+    dom = "phase1" if rmx["p1"] >= rmx["p2"] else "phase2"
+    dom_ms = rmx["p1"] if dom == "phase1" else rmx["p2"]
+    achieved = slice_products * 2.0 * k * el[dom] / (dom_ms * 1e-3) / 1e12
+    dom64 = "phase1" if r64["p1"] >= r64["p2"] else "phase2"
+    dom64_ms = r64["p1"] if dom64 == "phase1" else r64["p2"]
+    achieved64 = 2.0 * k * el[dom64] / (dom64_ms * 1e-3) / 1e12
+    # DRAM traffic / algorithmic bytes of the FP64 phases, measured by ncu on
+    # the n = 16384 instance (profiles/matmat_fp64_gemm_n16384_k256.md)
+    traffic_ratio64 = {"phase1": 1.31, "phase2": 1.14}
+    bytes64 = {"phase1": 8.0 * sn + 8.0 * n * k, "phase2": 8.0 * (leaves_el + sn) + 16.0 * n * k}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         res = run_cpu_baseline(args.cpu_n, k)
@@ -340,31 +392,42 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "precision": "fp64",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "s8 slices -> s32 on tensor cores (6 slices, 21 products), f64 result",
+        "data": "synthetic", "precision": "mixed",
         "config": {"workload": WORKLOAD, "n": n, "height": h, "leaf": n // (1 << h), "k": k,
                    "tol": tol, "kernel": "matern32 l=0.1 +1e-2 I, 2D Morton points seed 1",
                    "l2": "inputs larger than L2 (factors + X > 126 MB), no flush",
                    "parallelism": f"replicas{world}"},
         "build_s": build_s,
         "rel_err_vs_dense": rel_err,
+        "rel_err_mixed_vs_fp64": rel_err_mixed_vs_fp64,
         "tree": {"max_rank": info["max_rank"], "storage_doubles": storage,
                  "ranks_by_depth": [int(max(ranks[2 * ((1 << d) - 1):2 * ((1 << (d + 1)) - 1)]))
                                     for d in range(h)]},
         "gflops": flops_step / (ms_step * 1e-3) / 1e9,
-        "roofline": {"bound": "fp64", "kernel": f"gemm_f64_kernel ({dom})", "achieved": achieved,
-                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": traffic_ratio[dom] * phase[dom]["bytes"],
-                     "traffic_note": "ncu dram bytes/algorithmic bytes at n=16384, scaled",
-                     "algorithmic_bytes": phase[dom]["bytes"],
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-                     "phase_ms": {p: phase[p]["ms"] for p in phase},
-                     "phase_tflops": {p: phase[p]["flops"] / (phase[p]["ms"] * 1e-3) / 1e12
-                                      for p in phase}},
-        "clocks": clk.summary(),
+        "roofline": {"bound": "tensor", "kernel": f"ozaki_gemm_kernel ({dom})",
+                     "achieved": achieved, "peak": peak_i8, "unit": "TOPS (int8)",
+                     "frac": achieved / peak_i8, "traffic": None,
+                     "peak_source": peak_src,
+                     "phase_ms": {"phase1": rmx["p1"], "phase2": rmx["p2"]}},
+        "fp64": {"value": value_fp64, "unit": "GB/s", "ms_per_step": r64["ms"],
+                 "gflops": flops_step / (r64["ms"] * 1e-3) / 1e9,
+                 "e2e": bytes_step / e2e_s_fp64 / 1e9,
+                 "roofline": {"bound": "fp64", "kernel": f"gemm_f64_kernel ({dom64})",
+                              "achieved": achieved64, "peak": peak64, "unit": "TFLOP/s",
+                              "frac": achieved64 / peak64,
+                              "traffic": traffic_ratio64[dom64] * bytes64[dom64],
+                              "algorithmic_bytes": bytes64[dom64],
+                              "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                              "phase_ms": {"phase1": r64["p1"], "phase2": r64["p2"]}},
+                 "gpu_launches": r64["launches"]},
+        "speedup_mixed_vs_fp64": r64["ms"] / rmx["ms"],
+        "clocks": rmx["clocks"],
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": int(8 * n * k),
-                "d2h_bytes_per_step": int(8 * n * k), "ms_per_step": e2e_s * 1e3},
-        "gpu_launches": int(launches),
+                "d2h_bytes_per_step": int(8 * n * k), "ms_per_step": e2e_s * 1e3,
+                "path": "multiply_hodlr_dense, option matmat_precision=1"},
+        "gpu_launches": rmx["launches"],
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))

@@ -132,6 +132,7 @@ B200_API = {
     "hodlr_b200_set_host_allocator": (None, [VP, VP]),
     "hodlr_b200_phase_times": (C.c_int, [DP, C.c_int]),
     "hodlr_b200_build_stats": (C.c_int, [DP, C.c_int]),
+    "hodlr_b200_check": (C.c_int, [VP, VP]),
     "hodlr_b200_matvec_noalloc_dev": (C.c_int, [VP, VP, VP, VP]),
     "hodlr_b200_kernel_matrix_dev": (
         C.c_int, [VP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, VP, C.c_int, VP]),

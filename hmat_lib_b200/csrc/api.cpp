@@ -95,7 +95,14 @@ void host_product(DeviceTree &t, ProdOp op, const double *X, long long xr, long 
   DevBuf dx(xr * xc, s), dy(xr * xc, s);
   h2d(dx.p, X, xr, xc, ldx, s);
   const int k = (int)(op == ProdOp::L ? xr : xc);
-  product_f64(t, op, dx.p, k, xr, dy.p, xr, s);
+  // option "matmat_precision" = 1 routes H X through the int8 tensor-core
+  // path (about 42 bits); the default keeps FP64 throughout
+  bool aligned = true;
+  for (int m : t.g.leaf_m) aligned = aligned && (m % 32 == 0);
+  if (op == ProdOp::N && aligned && option("matmat_precision", 0.0) == 1.0)
+    product_mixed(t, dx.p, k, xr, dy.p, xr, s);
+  else
+    product_f64(t, op, dx.p, k, xr, dy.p, xr, s);
   d2h(Y, ldy, dy.p, xr, xc, s);
   HB_CUDA(cudaStreamSynchronize(s));
 }
@@ -429,7 +436,13 @@ int hodlr_b200_matmat_dev(hodlr_b200_tree t, int op, int precision, const double
                           int ldx, double *d_y, int ldy, void *stream) {
   if (!t || !d_x || !d_y || op < 0 || op > 2) return INPUT_ERROR;
   try {
-    HB_REQUIRE(precision == HODLR_B200_FP64, INPUT_ERROR, "precision mode not available");
+    if (precision == HODLR_B200_MIXED) {
+      HB_REQUIRE(op == HODLR_B200_OP_N, INPUT_ERROR,
+                 "mixed precision is available for Y = H X (op N)");
+      product_mixed(*t->p, d_x, k, ldx, d_y, ldy, as_stream(stream));
+      return SUCCESS;
+    }
+    HB_REQUIRE(precision == HODLR_B200_FP64, INPUT_ERROR, "unknown precision mode");
     product_f64(*t->p, (ProdOp)op, d_x, k, ldx, d_y, ldy, as_stream(stream));
     return SUCCESS;
   } catch (const Error &e) {
@@ -455,6 +468,19 @@ int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshol
 }
 
 int hodlr_b200_phase_times(double *out, int capacity) { return phase_times(out, capacity); }
+
+int hodlr_b200_check(hodlr_b200_tree t, void *stream) {
+  if (!t) return INPUT_ERROR;
+  try {
+    if (mixed_status(*t->p, as_stream(stream)) != 0) {
+      set_last_error("a mixed-precision kernel gave up waiting on a barrier");
+      return SVD_FAILURE;
+    }
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
 
 int hodlr_b200_build_stats(double *out, int capacity) {
   const BuildStats &st = last_build_stats();

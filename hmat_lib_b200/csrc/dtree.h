@@ -15,6 +15,7 @@
 namespace hb {
 
 struct ProductPlan;
+struct MixedState;
 
 struct DeviceTree {
   int device = 0;
@@ -27,6 +28,7 @@ struct DeviceTree {
   uint64_t fingerprint = 0;         // of the host tree this mirrors (0: none)
   std::map<std::tuple<int, int, long long, long long, int, int>, std::unique_ptr<ProductPlan>> plans;
   std::mutex plan_mutex;
+  std::shared_ptr<MixedState> mixed;   // int8 slices of the factors (mixed precision)
 
   DeviceTree() = default;
   DeviceTree(const DeviceTree &) = delete;

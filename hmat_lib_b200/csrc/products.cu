@@ -143,6 +143,22 @@ void collect_phase_times() {
 }
 }  // namespace
 
+PhaseTimer::PhaseTimer(cudaStream_t s) : stream(s) {
+  on = option("record_phase_times", 0.0) != 0.0;
+  if (!on) return;
+  for (auto &ev : e) HB_CUDA(cudaEventCreate(&ev));
+  HB_CUDA(cudaEventRecord(e[0], stream));
+}
+
+void PhaseTimer::mark(int i) {
+  if (!on) return;
+  HB_CUDA(cudaEventRecord(e[i], stream));
+  if (i == 2) {
+    std::lock_guard<std::mutex> lk(g_pt_mutex);
+    g_pending.push_back(PhaseEvents{{e[0], e[1], e[2]}});
+  }
+}
+
 int phase_times(double *out, int cap) {
   std::lock_guard<std::mutex> lk(g_pt_mutex);
   collect_phase_times();
@@ -165,20 +181,11 @@ void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx
   bases.p[kW] = plan.w;
   bases.p[4] = t.arena;
   bases.p[5] = t.arena;
-  const bool timed = option("record_phase_times", 0.0) != 0.0;
-  PhaseEvents pe{};
-  if (timed) {
-    for (auto &ev : pe.e) HB_CUDA(cudaEventCreate(&ev));
-    HB_CUDA(cudaEventRecord(pe.e[0], stream));
-  }
+  PhaseTimer timer(stream);
   gemm_plan_run(plan.phase1, bases, stream);
-  if (timed) HB_CUDA(cudaEventRecord(pe.e[1], stream));
+  timer.mark(1);
   gemm_plan_run(plan.phase2, bases, stream);
-  if (timed) {
-    HB_CUDA(cudaEventRecord(pe.e[2], stream));
-    std::lock_guard<std::mutex> lk(g_pt_mutex);
-    g_pending.push_back(pe);
-  }
+  timer.mark(2);
 }
 
 }  // namespace hb

@@ -48,6 +48,22 @@ ProductWork product_work(const DeviceTree &t, int k);
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
                  long long ldy, cudaStream_t stream, int min_depth = 0);
 
+// Mixed-precision Y = H X (op N) on the int8 tensor cores (products_mixed.cu).
+void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double *Y,
+                   long long ldy, cudaStream_t stream);
+// Error word of the tree's mixed-precision kernels (0: none), read and reset.
+int mixed_status(DeviceTree &t, cudaStream_t stream);
+
+// Events around the two phases of a product when option
+// "record_phase_times" is set (mark(1) after phase 1, mark(2) at the end).
+struct PhaseTimer {
+  cudaStream_t stream;
+  bool on = false;
+  cudaEvent_t e[3] = {};
+  explicit PhaseTimer(cudaStream_t s);
+  void mark(int i);
+};
+
 // Accumulated per-phase device times (ms) of products run with option
 // "record_phase_times" set: out[0] phase 1, out[1] phase 2, out[2] count.
 // Resets the accumulators.

@@ -67,6 +67,10 @@ int hodlr_b200_tree_ranks(hodlr_b200_tree t, int *ranks, int capacity);
 /* Y = op(H, X) on device buffers (column-major). */
 int hodlr_b200_matmat_dev(hodlr_b200_tree t, int op, int precision, const double *d_x, int k,
                           int ldx, double *d_y, int ldy, void *stream);
+/* Synchronises with `stream` and returns SUCCESS, or SVD_FAILURE if a
+ * mixed-precision kernel on this tree stopped on its bounded barrier wait
+ * since the last check (the error word is then reset). */
+int hodlr_b200_check(hodlr_b200_tree t, void *stream);
 /* H1 * H2 with recompression at svd_threshold, result stays on the device. */
 int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshold,
                        hodlr_b200_tree *out, int *ierr);
