@@ -436,6 +436,9 @@ int hodlr_b200_matmat_dev(hodlr_b200_tree t, int op, int precision, const double
                           int ldx, double *d_y, int ldy, void *stream) {
   if (!t || !d_x || !d_y || op < 0 || op > 2) return INPUT_ERROR;
   try {
+    const long long rows = (op == HODLR_B200_OP_L) ? k : t->p->g.n;
+    HB_REQUIRE(k >= 0 && ldx >= std::max(1LL, rows) && ldy >= std::max(1LL, rows), INPUT_ERROR,
+               "leading dimension below the number of rows");
     if (precision == HODLR_B200_MIXED) {
       HB_REQUIRE(op == HODLR_B200_OP_N, INPUT_ERROR,
                  "mixed precision is available for Y = H X (op N)");

@@ -1,19 +1,26 @@
-// int8-sliced FP64 products on tcgen05 (see ozaki.h for the scheme).
+// int8-sliced FP64 products on tcgen05 (see ozaki.h for the scheme and the
+// blocked operand layout).
 //
-// One CTA of 128 threads per 128 x 64 output tile.  The tile's K range is a
-// list of segments, each with its own row / column scaling; K advances 64
-// bytes per stage through a three-stage cp.async ring.  Thread 0 issues the
-// S(S+1)/2 slice products of every 32-byte k-step into S int32 TMEM
-// accumulators (group t = p + q - 2, 64 columns each) and commits each stage
-// to that stage's mbarrier, which frees the buffer for the next load.  At the
-// end of a segment the four warps read their 32 TMEM lanes, recombine the
-// groups in FP64 and add them, scaled by 2^(e_r + f_j), to 64 FP64 registers
-// per thread; the tile is written once (or added atomically for split K).
-//
-// Shared-memory operand layout: no swizzle, K-major, 8-row x 16-byte core
-// matrices; within a 64-byte stage a row group of 8 rows holds its four
-// K-chunks at 128-byte steps (leading byte offset 128) and successive row
-// groups are 512 bytes apart (stride byte offset 512).
+// Persistent kernel, one CTA of six warps per SM, tiles taken round-robin:
+//   warp 0 (one thread)  producer: per K-block one bulk copy of the A block
+//                        (all S slices of 128 lines) and one of the B block
+//                        into a six-stage ring, completion on full[stage];
+//   warp 1 (one thread)  MMA issuer: per K-block the S(S+1)/2 slice products
+//                        as 8 MMAs (slice p of A against slices q = 1 .. S+1-p
+//                        of B, which sit next to each other in shared memory,
+//                        so one MMA of N = (S+1-p) nw covers accumulator groups
+//                        t = p + q - 2 stored side by side in TMEM), commit to
+//                        empty[stage]; after the tile's last K-block a commit
+//                        to tmem_full;
+//   warps 2-5            epilogue: wait tmem_full, read the S int32 groups of
+//                        their 32 TMEM lanes, recombine in FP64, scale by
+//                        2^(e_r + f_j), release the accumulators (tmem_empty),
+//                        store or atomically add the tile.
+// The warp also owns the TMEM allocation (512 columns: S groups of <= 64).
+// Every barrier wait is bounded; a wait that runs out sets the CTA's abort
+// flag, every role leaves its loop, the producer waits (bounded) for its
+// copies in flight, the MMA thread for its MMAs, and the kernel reports
+// status 1 and returns.
 #include <algorithm>
 #include <cmath>
 
@@ -24,52 +31,45 @@ namespace hb {
 
 namespace {
 
-constexpr int kOzThreads = 128;
-constexpr int kASlice = kOzM * kOzKStage;          // bytes of one A slice per stage
-constexpr int kBSlice = kOzN * kOzKStage;          // bytes of one B slice per stage
-constexpr int kStageBytes = kOzSlices * (kASlice + kBSlice);
-constexpr size_t kOzSmem = (size_t)kOzStages * kStageBytes;
-constexpr long long kWaitTries = 1LL << 26;         // bounded barrier waits
+constexpr int kThreads = 192;
+constexpr int kStages = 6;
+constexpr int kStageBytes = kOzABlock + oz_bblock(kOzMaxNw);   // 36864
+constexpr size_t kSmem = (size_t)kStages * kStageBytes;        // 221184
+constexpr long long kWaitTries = 1LL << 26;
+constexpr int kSliceBytesA = kOzRowsA * kOzKBlock;              // 4096: one slice of an A block
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  const int bytes = pred ? 16 : 0;
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
-__device__ __forceinline__ int core_off(int row, int chunk) {
-  return (row >> 3) * 512 + chunk * 128 + (row & 7) * 16;
+// Bounded wait that also gives up when another role has aborted.
+__device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, volatile int *bad) {
+  for (long long i = 0; i < kWaitTries; ++i) {
+    if (umma::mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 255 && *bad) return false;
+  }
+  return false;
 }
 
-struct Cursor {
-  int seg;   // absolute segment index
-  int k0;    // byte offset of the stage inside the segment
-};
-
-__global__ void __launch_bounds__(kOzThreads, 1)
-ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ tiles, double *cbase,
-                  int *status) {
+__global__ void __launch_bounds__(kThreads, 1)
+ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ tiles, int ntiles,
+                  double *cbase, int *status) {
   extern __shared__ __align__(1024) uint8_t sm[];
-  __shared__ __align__(8) uint64_t bars[kOzStages];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ __align__(8) uint64_t empty[kStages];
+  __shared__ __align__(8) uint64_t tmem_full, tmem_empty, mma_done;
   __shared__ uint32_t taddr_s;
-  __shared__ int bad;
+  __shared__ volatile int bad;
 
-  const OzTile T = tiles[blockIdx.x];
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int seg_end = T.seg0 + T.nseg;
-
-  int nst = 0;
-  for (int s = T.seg0; s < seg_end; ++s) nst += (segs[s].K + kOzKStage - 1) / kOzKStage;
-
-  if (warp == 0) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 1) {
     umma::tmem_alloc(&taddr_s, 512);
     umma::tmem_relinquish();
   }
   if (tid == 0) {
-    for (int s = 0; s < kOzStages; ++s) umma::mbar_init(&bars[s], 1);
+    for (int s = 0; s < kStages; ++s) {
+      umma::mbar_init(&full[s], 1);
+      umma::mbar_init(&empty[s], 1);
+    }
+    umma::mbar_init(&tmem_full, 1);
+    umma::mbar_init(&tmem_empty, 4);
+    umma::mbar_init(&mma_done, 1);
     umma::fence_mbar_init();
     bad = 0;
   }
@@ -78,206 +78,216 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
   umma::fence_after_sync();
   const uint32_t tbase = taddr_s;
 
-  auto settle = [&](Cursor &c) {
-    while (c.seg < seg_end && c.k0 >= segs[c.seg].K) {
-      ++c.seg;
-      c.k0 = 0;
-    }
-  };
-  auto advance = [&](Cursor &c) {
-    c.k0 += kOzKStage;
-    settle(c);
-  };
-  auto load_stage = [&](int buf, const Cursor &c) {
-    const OzSeg G = segs[c.seg];
-    uint8_t *st = sm + buf * kStageBytes;
-    for (int e = tid; e < kOzSlices * kOzM * 4; e += kOzThreads) {
-      const int p = e / (kOzM * 4), rem = e % (kOzM * 4), r = rem >> 2, ch = rem & 3;
-      const int kb = c.k0 + ch * 16;
-      const bool ok = r < T.rows && kb < G.K;
-      const int8_t *src = G.a.base + p * G.a.slice_stride + (long long)r * G.a.ld + kb;
-      cp_async16(st + p * kASlice + core_off(r, ch), ok ? (const void *)src : (const void *)G.a.base,
-                 ok);
-    }
-    uint8_t *stb = st + kOzSlices * kASlice;
-    for (int e = tid; e < kOzSlices * kOzN * 4; e += kOzThreads) {
-      const int q = e / (kOzN * 4), rem = e % (kOzN * 4), n = rem >> 2, ch = rem & 3;
-      const int kb = c.k0 + ch * 16;
-      const bool ok = n < T.cols && kb < G.K;
-      const int8_t *src = G.b.base + q * G.b.slice_stride + (long long)n * G.b.ld + kb;
-      cp_async16(stb + q * kBSlice + core_off(n, ch), ok ? (const void *)src : (const void *)G.b.base,
-                 ok);
-    }
-  };
-
-  double acc[kOzN];
-#pragma unroll
-  for (int j = 0; j < kOzN; ++j) acc[j] = 0.0;
-
-  Cursor ld{T.seg0, 0}, mc{T.seg0, 0};
-  settle(ld);
-  settle(mc);
-  // prologue: two stages in flight
-  for (int i = 0; i < 2; ++i) {
-    if (i < nst) {
-      load_stage(i % kOzStages, ld);
-      advance(ld);
-    }
-    cp_async_commit();
-  }
-  constexpr uint32_t idesc = umma::idesc_s8(kOzM, kOzN);
-  uint32_t inited = 0;   // accumulator groups written in the current segment (thread 0)
-
-  for (int i = 0; i < nst; ++i) {
-    const int buf = i % kOzStages;
-    cp_async_wait1();
-    umma::fence_proxy_async();
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (bad) break;
-    const OzSeg G = segs[mc.seg];
-    if (tid == 0) {
-      const uint32_t sbase = umma::smem_u32(sm + buf * kStageBytes);
-      for (int ks = 0; ks < kOzKStage / 32; ++ks) {
-        if (mc.k0 + ks * 32 >= G.K) break;
-#pragma unroll
-        for (int p = 1; p <= kOzSlices; ++p)
-#pragma unroll
-          for (int q = 1; p + q <= kOzSlices + 1; ++q) {
-            const int t = p + q - 2;
-            const uint64_t ad =
-                umma::smem_desc_noswizzle(sbase + (p - 1) * kASlice + ks * 256, 128, 512);
-            const uint64_t bd = umma::smem_desc_noswizzle(
-                sbase + kOzSlices * kASlice + (q - 1) * kBSlice + ks * 256, 128, 512);
-            umma::mma_s8(tbase + t * kOzN, ad, bd, idesc, (inited >> t) & 1u);
-            inited |= 1u << t;
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      long long g = 0;   // K-blocks issued by this CTA
+      for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
+        const OzTile T = tiles[tile];
+        const uint32_t bbytes = (uint32_t)oz_bblock(T.nw);
+        for (int s = T.seg0; s < T.seg0 + T.nseg && !bad; ++s) {
+          const OzSeg G = segs[s];
+          for (int kb = 0; kb < G.nkb; ++kb) {
+            const int st = (int)(g % kStages);
+            const long long use = g / kStages;
+            if (use > 0 && !wait_or_abort(&empty[st], (uint32_t)((use - 1) & 1), &bad)) {
+              bad = 1;
+              break;
+            }
+            uint8_t *dst = sm + st * kStageBytes;
+            umma::mbar_expect_tx(&full[st], (uint32_t)kOzABlock + bbytes);
+            umma::bulk_g2s(dst, G.a + (long long)kb * kOzABlock, kOzABlock, &full[st]);
+            umma::bulk_g2s(dst + kOzABlock, G.b + (long long)kb * bbytes, bbytes, &full[st]);
+            ++g;
           }
-      }
-      umma::mma_commit(&bars[buf]);
-    }
-    // refill the buffer last used by stage i - 1 with stage i + 2
-    if (i + 2 < nst) {
-      if (i >= 1) {
-        const int pb = (i - 1) % kOzStages;
-        if (!umma::mbar_wait_bounded(&bars[pb], ((i - 1) / kOzStages) & 1, kWaitTries)) bad = 1;
-      }
-      if (!bad) {
-        load_stage((i + 2) % kOzStages, ld);
-        advance(ld);
-      }
-    }
-    cp_async_commit();
-    // end of a segment: recombine its accumulators into the FP64 registers
-    Cursor nx = mc;
-    advance(nx);
-    if (nx.seg != mc.seg) {
-      if (!umma::mbar_wait_bounded(&bars[buf], (i / kOzStages) & 1, kWaitTries)) bad = 1;
-      umma::fence_after_sync();
-      const int r = tid;
-      const int er = (r < T.rows) ? G.a.exp[r] : 0;
-      const uint32_t lane_addr = tbase + ((uint32_t)(32 * warp) << 16);
-#pragma unroll
-      for (int c0 = 0; c0 < kOzN; c0 += 16) {
-        double part[16];
-#pragma unroll
-        for (int x = 0; x < 16; ++x) part[x] = 0.0;
-        // every group was written: a drained segment has at least one k-step
-#pragma unroll
-        for (int t = 0; t < kOzSlices; ++t) {
-          int32_t v[16];
-          umma::tmem_ld16(lane_addr + t * kOzN + c0, v);
-          umma::tmem_ld_wait();
-          const double sc = ldexp(1.0, -7 * (t + 2));
-#pragma unroll
-          for (int x = 0; x < 16; ++x) part[x] = fma((double)v[x], sc, part[x]);
         }
+      }
+      // copies still in flight land before the CTA may exit
+      for (long long q = std::max(0LL, g - kStages); q < g; ++q)
+        umma::mbar_wait_bounded(&full[q % kStages], (uint32_t)((q / kStages) & 1), kWaitTries);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      long long g = 0;
+      int lt = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < ntiles && ok && !bad; tile += gridDim.x, ++lt) {
+        const OzTile T = tiles[tile];
+        if (lt > 0 && !wait_or_abort(&tmem_empty, (uint32_t)((lt - 1) & 1), &bad)) {
+          ok = false;
+          break;
+        }
+        umma::fence_after_sync();
+        const int nw = T.nw;
+        const int maxcnt = min(kOzSlices, 256 / nw);
+        const uint32_t bslice = (uint32_t)nw * kOzKBlock;
+        bool first = true;
+        for (int s = T.seg0; s < T.seg0 + T.nseg && ok; ++s) {
+          const int nkb = segs[s].nkb;
+          for (int kb = 0; kb < nkb; ++kb, ++g) {
+            const int st = (int)(g % kStages);
+            if (!wait_or_abort(&full[st], (uint32_t)((g / kStages) & 1), &bad)) {
+              ok = false;
+              break;
+            }
+            umma::fence_after_sync();
+            const uint32_t sa = umma::smem_u32(sm + st * kStageBytes);
+            const uint32_t sb = sa + kOzABlock;
 #pragma unroll
-        for (int x = 0; x < 16; ++x) {
-          const int j = c0 + x;
-          const int fj = (j < T.cols) ? G.b.exp[j] : 0;
-          acc[j] += ldexp(part[x], er + fj);
+            for (int p = 1; p <= kOzSlices; ++p) {
+              const uint64_t ad = umma::smem_desc_noswizzle(sa + (p - 1) * kSliceBytesA, 128, 256);
+              for (int q0 = 1; q0 <= kOzSlices + 1 - p;) {
+                const int cnt = min(kOzSlices + 2 - p - q0, maxcnt);
+                const uint64_t bd = umma::smem_desc_noswizzle(sb + (q0 - 1) * bslice, 128, 256);
+                umma::mma_s8(tbase + (uint32_t)((p + q0 - 2) * nw), ad, bd,
+                             umma::idesc_s8(kOzRowsA, cnt * nw), (first && p == 1) ? 0u : 1u);
+                q0 += cnt;
+              }
+            }
+            first = false;
+            umma::mma_commit(&empty[st]);
+          }
+        }
+        if (ok) umma::mma_commit(&tmem_full);
+      }
+      if (!ok) bad = 1;
+      // every MMA issued so far completes before the accumulators are freed
+      umma::mma_commit(&mma_done);
+      umma::mbar_wait_bounded(&mma_done, 0, kWaitTries);
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    const int quarter = warp & 3;   // TMEM lanes 32 quarter .. 32 quarter + 31
+    const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+    const int r = 32 * quarter + lane;
+    int lt = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++lt) {
+      if (__any_sync(0xffffffffu, bad)) break;
+      const OzTile T = tiles[tile];
+      const bool ready = wait_or_abort(&tmem_full, (uint32_t)(lt & 1), &bad);
+      if (!__all_sync(0xffffffffu, ready)) {
+        bad = 1;
+        break;
+      }
+      umma::fence_after_sync();
+      const int nw = T.nw;
+      const bool row_ok = r < T.rows;
+      const int er = row_ok ? T.rexp[r] : 0;
+      double *crow = cbase + T.c_off + r;
+      for (int c0 = 0; c0 < nw; c0 += 16) {
+        int32_t v[kOzSlices][16];
+#pragma unroll
+        for (int t = 0; t < kOzSlices; ++t) umma::tmem_ld16(lane_addr + t * nw + c0, v[t]);
+        umma::tmem_ld_wait();
+        if (row_ok) {
+#pragma unroll
+          for (int x = 0; x < 16; ++x) {
+            const int j = c0 + x;
+            if (j >= T.cols) break;
+            // sum_t v_t 2^(-7 t), then the common factor 2^(e_r + f_j - 14)
+            double acc = (double)v[kOzSlices - 1][x];
+#pragma unroll
+            for (int t = kOzSlices - 2; t >= 0; --t) acc = fma(acc, 0x1p-7, (double)v[t][x]);
+            const double val = ldexp(acc, er + T.cexp[j] - 14);
+            double *c = crow + (long long)j * T.ldc;
+            if (T.atomic)
+              atomicAdd(c, val);
+            else
+              *c = val;
+          }
         }
       }
       umma::fence_before_sync();
-      __syncthreads();
-      if (tid == 0) inited = 0;
+      __syncwarp();
+      if (lane == 0) umma::mbar_arrive(&tmem_empty);
     }
-    mc = nx;
   }
-  cp_async_wait0();
 
-  if (!bad && tid < T.rows) {
-    const int r = tid;
-#pragma unroll
-    for (int j = 0; j < kOzN; ++j) {
-      if (j >= T.cols) continue;
-      double *c = cbase + T.c_off + r + (long long)j * T.ldc;
-      if (T.atomic)
-        atomicAdd(c, acc[j]);
-      else
-        *c = acc[j];
-    }
-  }
-  if (bad && tid == 0) {
-    atomicExch(status, 1);
-    // let any MMA still in flight finish before the TMEM is released
-    for (int s = 0; s < kOzStages; ++s) umma::mbar_wait_bounded(&bars[s], 0, kWaitTries);
-  }
+  __syncwarp();
   umma::fence_before_sync();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tbase, 512);
+  if (bad && tid == 0) atomicExch(status, 1);
+  if (warp == 1) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tbase, 512);
+  }
 }
 
-// ---- slicing ---------------------------------------------------------------------
+// ---- exponents and slicing ---------------------------------------------------------
 
-__device__ __forceinline__ int scale_exponent(double maxabs) {
+__device__ __forceinline__ int scale_exponent(unsigned long long bits) {
+  const double maxabs = __longlong_as_double((long long)bits);
   if (!(maxabs > 0.0)) return 0;
   int e;
   const double mant = frexp(maxabs, &e);   // maxabs = mant 2^e, mant in [0.5, 1)
   return mant > 127.0 / 128.0 ? e + 1 : e;
 }
 
-// exponent per row (rowwise) or per column (colwise) of the source
-__global__ void slice_exp_kernel(const SliceJob *__restrict__ jobs) {
-  const SliceJob J = jobs[blockIdx.y];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int count = J.rowwise ? J.m : J.k;
-  for (int v = blockIdx.x * nw + warp; v < count; v += gridDim.x * nw) {
-    double mx = 0.0;
-    if (J.rowwise) {
-      for (int c = lane; c < J.k; c += 32) mx = fmax(mx, fabs(J.src[v + (long long)c * J.ld]));
-    } else {
-      const double *col = J.src + (long long)v * J.ld;
-      for (int r = lane; r < J.m; r += 32) mx = fmax(mx, fabs(col[r]));
-    }
+template <class Job>
+__device__ __forceinline__ int find_job(const Job *jobs, int njobs, long long item) {
+  int lo = 0, hi = njobs - 1;   // last job with item0 <= item
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].item0 <= item)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Work items are warps: a line (K contiguous: lanes split K) or 32 lines (one
+// per lane, loop over K).
+__global__ void max_kernel(const MaxJob *__restrict__ jobs, int njobs, long long items,
+                           const double *xbase) {
+  const int lane = threadIdx.x & 31;
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long it = w0; it < items; it += nw) {
+    const MaxJob &J = jobs[find_job(jobs, njobs, it)];
+    const double *src = J.src ? J.src : xbase;
+    const long long local = it - J.item0;
+    if (J.s_k == 1) {
+      const double *row = src + local * J.s_line;
+      double mx = 0.0;
+      for (int k = lane; k < J.K; k += 32) mx = fmax(mx, fabs(row[k]));
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) J.exp[v] = scale_exponent(mx);
+      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (lane == 0 && mx > 0.0)
+        atomicMax(J.out + local, (unsigned long long)__double_as_longlong(mx));
+    } else {
+      const long long line = local * 32 + lane;
+      if (line < J.lines) {
+        double mx = 0.0;
+        const double *p = src + line * J.s_line;
+        for (int k = 0; k < J.K; ++k) mx = fmax(mx, fabs(p[(long long)k * J.s_k]));
+        if (mx > 0.0) atomicMax(J.out + line, (unsigned long long)__double_as_longlong(mx));
+      }
+    }
   }
 }
 
-// 16 consecutive K positions of one row (rowwise) or column (colwise) per
-// thread; every slice gets one aligned 16-byte store; padding is zero.
-__global__ void slice_kernel(const SliceJob *__restrict__ jobs) {
-  const SliceJob J = jobs[blockIdx.y];
-  const int lines = J.rowwise ? J.m : J.k;       // rows of the sliced operand
-  const int chunks = J.dld / 16;                 // 16-byte chunks per line (padded)
-  const long long total = (long long)lines * chunks;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int line = (int)(e % lines), ch = (int)(e / lines);
-    const int ex = J.exp[line];
+// One item = 16 consecutive K positions of one line: six aligned 16-byte
+// stores, one per slice.  Lines vary fastest, so eight neighbouring items
+// fill one 128-byte core matrix.
+__global__ void slice_kernel(const SliceJob *__restrict__ jobs, int njobs, long long items,
+                             const double *xbase) {
+  for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < items;
+       it += (long long)gridDim.x * blockDim.x) {
+    const SliceJob &J = jobs[find_job(jobs, njobs, it)];
+    const double *src = J.src ? J.src : xbase;
+    const long long local = it - J.item0;
+    const int L = J.ntiles * J.R;
+    const int line = (int)(local % L), c16 = (int)(local / L);
+    const bool live = line < J.lines;
+    const int ex = live ? scale_exponent(J.maxabs[line]) : 0;
+    if (J.exp_out && c16 == 0 && live) J.exp_out[line] = ex;
     int8_t out[kOzSlices][16];
 #pragma unroll
     for (int x = 0; x < 16; ++x) {
-      const int kk = ch * 16 + x;
-      double y = 0.0;
-      if (J.rowwise) {
-        if (kk < J.k) y = J.src[line + (long long)kk * J.ld];
-      } else {
-        if (kk < J.m) y = J.src[kk + (long long)line * J.ld];
-      }
+      const int k = c16 * 16 + x;
+      double y = (live && k < J.K) ? src[(long long)line * J.s_line + (long long)k * J.s_k] : 0.0;
       y = ldexp(y, -ex);
 #pragma unroll
       for (int p = 0; p < kOzSlices; ++p) {
@@ -287,13 +297,21 @@ __global__ void slice_kernel(const SliceJob *__restrict__ jobs) {
         y -= a;
       }
     }
+    const int t = line / J.R, lr = line % J.R;
+    uint8_t *base = J.dst + (long long)t * J.tile_stride +
+                    oz_offset(J.R, 0, lr, (J.kb0 * kOzKBlock) + c16 * 16);
 #pragma unroll
     for (int p = 0; p < kOzSlices; ++p) {
       int4 w;
       memcpy(&w, out[p], 16);
-      *reinterpret_cast<int4 *>(J.dst + p * J.slice_stride + (long long)line * J.dld + ch * 16) = w;
+      *reinterpret_cast<int4 *>(base + (long long)p * J.R * kOzKBlock) = w;
     }
   }
+}
+
+int grid_for(long long threads) {
+  const long long cap = (long long)num_sms() * 8;
+  return (int)std::max(1LL, std::min(cap, (threads + 255) / 256));
 }
 
 }  // namespace
@@ -304,31 +322,45 @@ void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *
   static bool configured = false;
   if (!configured) {
     HB_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kOzSmem));
+                                 (int)kSmem));
     configured = true;
   }
-  for (int off = 0; off < ntiles; off += 65535) {
-    const int cnt = std::min(65535, ntiles - off);
-    ozaki_gemm_kernel<<<cnt, kOzThreads, kOzSmem, stream>>>(d_segs, d_tiles + off, cbase,
-                                                             d_status);
-    HB_LAUNCHED();
-  }
+  const int grid = std::min(ntiles, num_sms());
+  ozaki_gemm_kernel<<<grid, kThreads, kSmem, stream>>>(d_segs, d_tiles, ntiles, cbase, d_status);
+  HB_LAUNCHED();
 }
 
-void ozaki_slice(const std::vector<SliceJob> &jobs, cudaStream_t stream) {
-  if (jobs.empty()) return;
-  SliceJob *d = nullptr;
-  HB_CUDA(cudaMallocAsync((void **)&d, sizeof(SliceJob) * jobs.size(), stream));
-  HB_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(SliceJob) * jobs.size(), cudaMemcpyHostToDevice,
-                          stream));
-  for (size_t off = 0; off < jobs.size(); off += 65535) {
-    dim3 grid(16, (unsigned)std::min<size_t>(65535, jobs.size() - off));
-    slice_exp_kernel<<<grid, 256, 0, stream>>>(d + off);
-    HB_LAUNCHED();
-    slice_kernel<<<grid, 256, 0, stream>>>(d + off);
-    HB_LAUNCHED();
+long long ozaki_prepare_max(std::vector<MaxJob> &jobs) {
+  long long items = 0;
+  for (auto &j : jobs) {
+    j.item0 = items;
+    items += (j.s_k == 1) ? j.lines : (j.lines + 31) / 32;
   }
-  cudaFreeAsync(d, stream);
+  return items;
+}
+
+long long ozaki_prepare_slice(std::vector<SliceJob> &jobs) {
+  long long items = 0;
+  for (auto &j : jobs) {
+    HB_REQUIRE(j.R % 8 == 0 && j.R >= 8, INPUT_ERROR, "slice tile lines");
+    j.item0 = items;
+    items += (long long)j.ntiles * j.R * j.nkb * 2;
+  }
+  return items;
+}
+
+void ozaki_max(const MaxJob *d_jobs, int njobs, long long items, const double *xbase,
+               cudaStream_t stream) {
+  if (njobs <= 0 || items <= 0) return;
+  max_kernel<<<grid_for(items * 32), 256, 0, stream>>>(d_jobs, njobs, items, xbase);
+  HB_LAUNCHED();
+}
+
+void ozaki_slice(const SliceJob *d_jobs, int njobs, long long items, const double *xbase,
+                 cudaStream_t stream) {
+  if (njobs <= 0 || items <= 0) return;
+  slice_kernel<<<grid_for(items), 256, 0, stream>>>(d_jobs, njobs, items, xbase);
+  HB_LAUNCHED();
 }
 
 }  // namespace hb

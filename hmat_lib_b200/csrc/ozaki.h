@@ -11,8 +11,18 @@
 // 7 new bits); columns of B likewise with 2^-f_j.  Then
 //   (A B)_rj ~= 2^(e_r + f_j) sum_{t=2}^{S+1} 2^(-7t) sum_{p+q=t} (a^(p) b^(q))_rj
 // keeping the S(S+1)/2 slice products with p + q <= S + 1.  Each inner sum is
-// one int32 TMEM accumulator (exact: |sum| < 2^31 for K <= 8192).  With S = 6
-// the truncation error is about 2^-42 relative to |A_r|_max |B_j|_max per term.
+// one int32 TMEM accumulator.  The largest group (p + q = S + 1) adds at most
+// 2*127*64 + 4*64*64 = 32640 per k, so the sums are exact for K <= 65536.
+// With S = 6 the truncation error is about 2^-42 relative to
+// |A_r|_max |B_j|_max per term.
+//
+// Operands live in global memory in the blocked layout the MMA reads from
+// shared memory, so one K-block of a tile is a single contiguous bulk copy:
+// a tile of R lines (rows of A, or columns of B) is a sequence of K-blocks of
+// 32 bytes; K-block = [slice 0..S-1][line / 8][k-chunk 0..1][line % 8][16
+// bytes of k] (no swizzle, K-major 8 x 16-byte core matrices: 128 bytes
+// between k-chunks, 256 bytes between 8-line groups, R * 32 bytes between
+// slices).
 #pragma once
 
 #include <cstdint>
@@ -22,60 +32,82 @@
 
 namespace hb {
 
-constexpr int kOzSlices = 6;         // S
-constexpr int kOzM = 128;            // tile rows (one MMA M)
-constexpr int kOzN = 64;             // tile columns (one MMA N)
-constexpr int kOzKStage = 64;        // K bytes per pipeline stage (2 MMA k-steps of 32)
-constexpr int kOzStages = 3;
-constexpr int kOzMaxK = 8192;        // K per tile and segment, keeps int32 exact
+constexpr int kOzSlices = 6;                                   // S
+constexpr int kOzKBlock = 32;                                  // K bytes per stage (one k-step)
+constexpr int kOzRowsA = 128;                                  // A tile lines (MMA M)
+constexpr int kOzMaxNw = 64;                                   // widest B tile
+constexpr int kOzABlock = kOzSlices * kOzRowsA * kOzKBlock;    // 24576 bytes
+constexpr int kOzMaxK = 65536;                                 // exact int32 group sums
 
-// int8 slices of one operand: slice p at base + p * slice_stride; element
-// (row, k) of an A-type operand at row * ld + k (rows K-major); element
-// (col, k) of a B-type operand at col * ld + k.  One exponent per row (A) or
-// column (B).
-struct OzOperand {
-  const int8_t *base;
-  long long slice_stride;
-  int ld;
-  const int *exp;
-};
+__host__ __device__ constexpr int oz_bblock(int nw) { return kOzSlices * nw * kOzKBlock; }
 
-// One K segment of a tile: A rows [0, rows) and B columns [0, cols) relative
-// to the descriptors' bases, K in [0, K) (K a multiple of 32; the slices are
-// zero-padded up to it).
+// Byte offset of element (line, k) of slice `p` inside a tile of R lines.
+__host__ __device__ inline long long oz_offset(int R, int p, int line, int k) {
+  return (long long)(k >> 5) * (kOzSlices * R * kOzKBlock) + (long long)p * R * kOzKBlock +
+         (line >> 3) * 256 + ((k >> 4) & 1) * 128 + (line & 7) * 16 + (k & 15);
+}
+
+// One K range of a tile: `nkb` K-blocks of A starting at `a` (kOzABlock bytes
+// each) against as many K-blocks of B starting at `b` (oz_bblock(nw) each).
 struct OzSeg {
-  OzOperand a, b;
-  int K;
+  const uint8_t *a;
+  const uint8_t *b;
+  int nkb;
+  int pad_;
 };
 
+// One 128 x nw output tile: the K segments seg0 .. seg0 + nseg - 1 all share
+// the row exponents rexp[0 .. rows) and column exponents cexp[0 .. cols), so
+// the tile is recombined once.  Element (r, j) goes to cbase[c_off + r + j ldc].
 struct OzTile {
   int seg0, nseg;
-  int rows, cols;   // valid extent of the output tile (<= 128 x 64)
-  long long c_off;  // output tile origin (column-major) relative to the launch's base
-  long long ldc;
-  int atomic;       // 1: atomically add into C (split K)
+  int rows, cols;
+  int nw;          // B tile width: multiple of 16, <= 64
+  int atomic;      // 1: add atomically (K split over several tiles)
+  long long c_off, ldc;
+  const int *rexp, *cexp;
 };
 
-// Runs the tiles (one CTA each).  `status` (device int) receives
-// SVD_FAILURE-style error code 1 if a bounded barrier wait ran out.
+// Runs all tiles with a persistent grid (one CTA per SM).  `status` (device
+// int) is set to 1 if a bounded barrier wait ran out.
 void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *cbase,
                 int *d_status, cudaStream_t stream);
 
-// Slicing.  `rowwise`: scale and slice the rows of a column-major m x k
-// matrix, write row-major slices (ld kpad) -> an A-type operand.
-// `colwise`: scale and slice the columns -> column-contiguous slices (ld
-// mpad) for a B-type operand, or for an A-type operand whose rows are the
-// columns (V^T).  shift: extra power of two applied to every value (exact).
+// Largest |value| per line of a strided FP64 matrix, element (line, k) at
+// src[line * s_line + k * s_k], combined by atomic max into out[line] (the
+// bit pattern of a non-negative double; zero it first).  A NULL src stands
+// for the `xbase` argument of the launch.  item0: prefix over the jobs of
+// their work items (filled by ozaki_prepare_max).
+struct MaxJob {
+  const double *src;
+  long long s_line, s_k;
+  int lines, K;
+  unsigned long long *out;
+  long long item0;
+};
+
+// Scales every line by its exponent (from maxabs[line]) and writes the int8
+// slices in the blocked layout: lines [0, ntiles R) (zero past `lines`),
+// K-blocks [kb0, kb0 + nkb) of each tile (zero past K).  exp_out, if set,
+// receives the exponent of every line.
 struct SliceJob {
   const double *src;
-  long long ld;
-  int m, k;          // source rows, columns
-  int8_t *dst;
-  long long slice_stride;
-  int dld;           // destination leading dimension (kpad for rowwise, mpad for colwise)
-  int *exp;          // exponents: m (rowwise) or k (colwise)
-  int rowwise;
+  long long s_line, s_k;
+  int lines, K;
+  int R, ntiles, kb0, nkb;
+  uint8_t *dst;
+  long long tile_stride;
+  const unsigned long long *maxabs;
+  int *exp_out;
+  long long item0;
 };
-void ozaki_slice(const std::vector<SliceJob> &jobs, cudaStream_t stream);
+
+// Fill item0 and return the total item count.
+long long ozaki_prepare_max(std::vector<MaxJob> &jobs);
+long long ozaki_prepare_slice(std::vector<SliceJob> &jobs);
+void ozaki_max(const MaxJob *d_jobs, int njobs, long long items, const double *xbase,
+               cudaStream_t stream);
+void ozaki_slice(const SliceJob *d_jobs, int njobs, long long items, const double *xbase,
+                 cudaStream_t stream);
 
 }  // namespace hb

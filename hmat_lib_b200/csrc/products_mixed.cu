@@ -1,63 +1,34 @@
 // Mixed-precision HODLR x dense product (op N) on the int8 tensor cores.
 //
-// Same two phases as the FP64 product (products.cu) with every GEMM done by
-// the sliced int8 kernel (ozaki.cu):
-//   1. W_b = V_b^T X_b for every block: A = V_b^T (rows = columns of V_b,
-//      scaled per column), B = X (scaled per column over all rows), split
-//      along n_b, partial tiles added atomically in FP64;
-//   2. Y[leaf] = D X[leaf] + sum_levels U_b[rows] W_b: one tile per leaf band
-//      and 64 columns, one K segment per term with its own scaling (D rows,
-//      U_b rows, X columns, W_b columns per block).
-// The slices of the tree's factors are made once and kept on the device;
-// X and W are sliced at every call.  Requires leaf sizes that are multiples
-// of 32 (16-byte aligned operand rows).
+// The FP64 product's two phases (products.cu), each one launch of the
+// sliced int8 kernel (ozaki.cu):
+//   1. W_b^T = X_b^T V_b for every block b: A = X^T (128 columns of X per
+//      tile, K = the block's rows of X), B = V_b (<= 64 columns per tile).
+//      Long blocks are split along K and added atomically in FP64.
+//   2. Y[band] = [D | U_{b_h-1}[band] | ... | U_{b_0}[band]] [X[band]; W_{b_h-1}; ...; W_{b_0}]
+//      for every 128-row band of every leaf and 64 columns of Y: one
+//      concatenated K range per tile, so the tile is recombined once.  Every
+//      row of the concatenated A shares one exponent (largest |entry| of the
+//      leaf row and of the U rows beside it), every column of the
+//      concatenated B one exponent (largest |entry| of that column of X and
+//      of all W_b).
+// Tree slices (A of phase 2, B of phase 1) are made once per tree; X is
+// sliced twice per call (with its own column exponents for phase 1, with
+// the common ones for phase 2) and W once.  Leaf sizes must be multiples of
+// 32 (whole K-blocks).
 #include <algorithm>
+#include <tuple>
 
 #include "ozaki.h"
 #include "products.h"
 
 namespace hb {
 
-struct MixedState {
-  int8_t *bytes = nullptr;
-  int *exps = nullptr;
-  std::vector<long long> d_off, u_off, v_off;   // byte offsets of slice 0
-  std::vector<long long> d_exp, u_exp, v_exp;   // int offsets
-  std::vector<int> kpad, spad;
-  std::map<std::pair<int, long long>, std::unique_ptr<struct MixedPlan>> plans;
-  ~MixedState();
-};
-
-struct MixedPlan {
-  int k = 0;
-  int8_t *xs = nullptr;      // X slices [S][k][n]
-  int *xe = nullptr;         // X column exponents [k]
-  double *w = nullptr;       // W (FP64)
-  int8_t *ws = nullptr;      // W slices, per block [S][k][spad_b]
-  int *we = nullptr;         // W exponents, per block [k]
-  std::vector<long long> w_off, ws_off, we_off;
-  OzSeg *seg1 = nullptr, *seg2 = nullptr;
-  OzTile *tile1 = nullptr, *tile2 = nullptr;
-  int ntile1 = 0, ntile2 = 0;
-  int *status = nullptr;
-  std::vector<SliceJob> wjobs;
-  ~MixedPlan() {
-    for (void *p : {(void *)xs, (void *)xe, (void *)w, (void *)ws, (void *)we, (void *)seg1,
-                    (void *)seg2, (void *)tile1, (void *)tile2, (void *)status})
-      if (p) cudaFree(p);
-  }
-};
-
-MixedState::~MixedState() {
-  plans.clear();
-  if (bytes) cudaFree(bytes);
-  if (exps) cudaFree(exps);
-}
-
 namespace {
 
-long long pad16(long long x) { return (x + 15) / 16 * 16; }
+int pad16(int x) { return (x + 15) / 16 * 16; }
 int pad32(int x) { return (x + 31) / 32 * 32; }
+long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
 
 template <class T>
 T *upload(const std::vector<T> &v, cudaStream_t s) {
@@ -68,6 +39,95 @@ T *upload(const std::vector<T> &v, cudaStream_t s) {
   return d;
 }
 
+template <class T>
+T *dalloc(long long count) {
+  T *d = nullptr;
+  HB_CUDA(cudaMalloc((void **)&d, sizeof(T) * std::max<long long>(count, 1)));
+  return d;
+}
+
+// Block of level d whose rows hold leaf i.
+int covering(int h, int i, int d) {
+  const int j = i >> (h - d);
+  const bool top = ((i >> (h - d - 1)) & 1) == 0;
+  return block_index(d, j, top ? 1 : 2);
+}
+
+// Every byte a segment, slice job or output tile touches lies inside the
+// buffer it belongs to (checked on the host when a plan is made).
+bool inside(const void *p, long long bytes, const void *base, long long size) {
+  auto *q = (const uint8_t *)p, *b = (const uint8_t *)base;
+  return bytes >= 0 && q >= b && q + bytes <= b + size;
+}
+
+void check_slice(const SliceJob &j, const void *buf, long long size) {
+  HB_REQUIRE(j.nkb > 0 && j.ntiles > 0, INPUT_ERROR, "mixed plan: empty slice job");
+  const long long last = (long long)(j.ntiles - 1) * j.tile_stride +
+                         oz_offset(j.R, kOzSlices - 1, j.R - 1, (j.kb0 + j.nkb) * kOzKBlock - 1);
+  HB_REQUIRE(inside(j.dst, last + 1, buf, size), INPUT_ERROR,
+             "mixed plan: slice job outside its buffer");
+}
+
+void check_seg(const OzSeg &g, int nw, const void *abuf, long long asize, const void *bbuf0,
+               long long bsize0, const void *bbuf1, long long bsize1) {
+  HB_REQUIRE(g.nkb > 0, INPUT_ERROR, "mixed plan: empty segment");
+  HB_REQUIRE(inside(g.a, (long long)g.nkb * kOzABlock, abuf, asize), INPUT_ERROR,
+             "mixed plan: A segment outside its buffer");
+  const long long bb = (long long)g.nkb * oz_bblock(nw);
+  HB_REQUIRE(inside(g.b, bb, bbuf0, bsize0) || inside(g.b, bb, bbuf1, bsize1), INPUT_ERROR,
+             "mixed plan: B segment outside its buffer");
+}
+
+}  // namespace
+
+struct MixedPlan;
+
+struct MixedState {
+  uint8_t *bytes = nullptr;                // phase-2 A bands, phase-1 B tiles
+  long long nbytes = 0;
+  int *exps = nullptr;                     // row exponents [n], V column exponents
+  unsigned long long *maxabs = nullptr;    // same layout, largest |entry|
+  std::vector<long long> band_off;         // per leaf: bytes of its first 128-row band
+  std::vector<int> band_nkb;               // per leaf: K-blocks of its concatenated row
+  std::vector<long long> vb_off;           // per block: bytes of its first B tile
+  std::vector<int> nw, ntn;                // per block: B tile width, number of tiles
+  std::vector<long long> gexp;             // per block: offset of its column exponents
+  std::map<std::tuple<int, long long, long long>, std::unique_ptr<MixedPlan>> plans;
+  ~MixedState();
+};
+
+struct MixedPlan {
+  int k = 0, nw2 = 0;
+  unsigned long long *xmax = nullptr, *fmax = nullptr;
+  int *xexp = nullptr, *fexp = nullptr;
+  uint8_t *xa = nullptr, *xb = nullptr, *wb = nullptr;
+  double *w = nullptr;
+  long long w_zero = 0;                    // leading doubles of w added to atomically
+  MaxJob *max_x = nullptr, *max_w = nullptr;
+  SliceJob *sl_x = nullptr, *sl_b = nullptr;
+  int n_max_w = 0, n_sl_b = 0;
+  long long it_max_x = 0, it_max_w = 0, it_sl_x = 0, it_sl_b = 0;
+  OzSeg *seg1 = nullptr, *seg2 = nullptr;
+  OzTile *tile1 = nullptr, *tile2 = nullptr;
+  int ntile1 = 0, ntile2 = 0;
+  int *status = nullptr;
+  ~MixedPlan() {
+    for (void *p : {(void *)xmax, (void *)fmax, (void *)xexp, (void *)fexp, (void *)xa, (void *)xb,
+                    (void *)wb, (void *)w, (void *)max_x, (void *)max_w, (void *)sl_x, (void *)sl_b,
+                    (void *)seg1, (void *)seg2, (void *)tile1, (void *)tile2, (void *)status})
+      if (p) cudaFree(p);
+  }
+};
+
+MixedState::~MixedState() {
+  plans.clear();
+  if (bytes) cudaFree(bytes);
+  if (exps) cudaFree(exps);
+  if (maxabs) cudaFree(maxabs);
+}
+
+namespace {
+
 MixedState &mixed_state(DeviceTree &t, cudaStream_t s) {
   if (t.mixed) return *t.mixed;
   const Geometry &g = t.g;
@@ -75,184 +135,272 @@ MixedState &mixed_state(DeviceTree &t, cudaStream_t s) {
     HB_REQUIRE(m % 32 == 0, INPUT_ERROR,
                "mixed precision needs leaf sizes that are multiples of 32");
   auto st = std::make_shared<MixedState>();
-  const int S = kOzSlices;
-  long long bytes = 0, ints = 0;
-  const int nl = g.nleaf(), nb = g.nblock();
-  st->d_off.resize(nl);
-  st->d_exp.resize(nl);
-  st->kpad.resize(nl);
+  const int nl = g.nleaf(), nb = g.nblock(), h = g.h, n = g.n;
+  long long bytes = 0, nexp = n;
+  st->band_off.resize(nl);
+  st->band_nkb.resize(nl);
   for (int i = 0; i < nl; ++i) {
-    const int m = g.leaf_m[i];
-    st->kpad[i] = pad32(m);
-    st->d_off[i] = bytes;
-    bytes += pad16((long long)S * m * st->kpad[i]);
-    st->d_exp[i] = ints;
-    ints += m;
+    int K = g.leaf_m[i];
+    for (int d = h - 1; d >= 0; --d) K += pad32(g.blocks[covering(h, i, d)].s);
+    HB_REQUIRE(K <= kOzMaxK, INPUT_ERROR, "mixed precision: leaf row plus ranks above 65536");
+    st->band_nkb[i] = K / kOzKBlock;
+    st->band_off[i] = bytes;
+    bytes += cdiv(g.leaf_m[i], kOzRowsA) * (long long)st->band_nkb[i] * kOzABlock;
   }
-  st->u_off.resize(nb);
-  st->v_off.resize(nb);
-  st->u_exp.resize(nb);
-  st->v_exp.resize(nb);
-  st->spad.resize(nb);
+  st->vb_off.assign(nb, 0);
+  st->nw.assign(nb, 0);
+  st->ntn.assign(nb, 0);
+  st->gexp.assign(nb, 0);
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
-    st->spad[b] = pad32(std::max(B.s, 1));
-    st->u_off[b] = bytes;
-    bytes += pad16((long long)S * B.m * st->spad[b]);
-    st->v_off[b] = bytes;
-    bytes += pad16((long long)S * B.s * pad32(B.n));
-    st->u_exp[b] = ints;
-    ints += B.m;
-    st->v_exp[b] = ints;
-    ints += B.s;
+    if (B.s == 0) continue;
+    st->ntn[b] = (int)cdiv(B.s, kOzMaxNw);
+    st->nw[b] = pad16((int)cdiv(B.s, st->ntn[b]));
+    st->vb_off[b] = bytes;
+    bytes += (long long)st->ntn[b] * (B.n / kOzKBlock) * oz_bblock(st->nw[b]);
+    st->gexp[b] = nexp;
+    nexp += B.s;
   }
-  HB_CUDA(cudaMalloc((void **)&st->bytes, std::max<long long>(bytes, 16)));
-  HB_CUDA(cudaMalloc((void **)&st->exps, sizeof(int) * std::max<long long>(ints, 1)));
-  HB_CUDA(cudaMemsetAsync(st->bytes, 0, std::max<long long>(bytes, 16), s));
-  std::vector<SliceJob> jobs;
+  st->bytes = dalloc<uint8_t>(bytes);
+  st->nbytes = bytes;
+  st->exps = dalloc<int>(nexp);
+  st->maxabs = dalloc<unsigned long long>(nexp);
+  HB_CUDA(cudaMemsetAsync(st->maxabs, 0, sizeof(unsigned long long) * nexp, s));
+
+  std::vector<MaxJob> mj;
+  std::vector<SliceJob> sj;
   for (int i = 0; i < nl; ++i) {
-    const int m = g.leaf_m[i];
-    if (m == 0) continue;
-    jobs.push_back(SliceJob{t.arena + t.leaves[i].off, m, m, m, st->bytes + st->d_off[i],
-                            (long long)m * st->kpad[i], st->kpad[i], st->exps + st->d_exp[i], 1});
+    const LeafDesc &L = t.leaves[i];
+    const int bands = (int)cdiv(L.m, kOzRowsA);
+    const long long stride = (long long)st->band_nkb[i] * kOzABlock;
+    const double *D = t.arena + L.off;
+    mj.push_back(MaxJob{D, 1, L.m, L.m, L.m, st->maxabs + L.r0, 0});
+    sj.push_back(SliceJob{D, 1, L.m, L.m, L.m, kOzRowsA, bands, 0, L.m / kOzKBlock,
+                          st->bytes + st->band_off[i], stride, st->maxabs + L.r0,
+                          st->exps + L.r0, 0});
+    int kb = L.m / kOzKBlock;
+    for (int d = h - 1; d >= 0; --d) {
+      const BlockDesc &B = g.blocks[covering(h, i, d)];
+      if (B.s == 0) continue;
+      const double *U = t.arena + B.u_off + (L.r0 - B.r0);
+      sj.push_back(SliceJob{U, 1, B.m, L.m, B.s, kOzRowsA, bands, kb, pad32(B.s) / kOzKBlock,
+                            st->bytes + st->band_off[i], stride, st->maxabs + L.r0, nullptr,
+                            0});
+      kb += pad32(B.s) / kOzKBlock;
+    }
   }
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
     if (B.s == 0) continue;
-    jobs.push_back(SliceJob{t.arena + B.u_off, B.m, B.m, B.s, st->bytes + st->u_off[b],
-                            (long long)B.m * st->spad[b], st->spad[b], st->exps + st->u_exp[b], 1});
-    jobs.push_back(SliceJob{t.arena + B.v_off, B.n, B.n, B.s, st->bytes + st->v_off[b],
-                            (long long)B.s * pad32(B.n), pad32(B.n), st->exps + st->v_exp[b], 0});
+    mj.push_back(MaxJob{t.arena + B.u_off, 1, B.m, B.m, B.s, st->maxabs + B.r0, 0});
+    const double *V = t.arena + B.v_off;
+    mj.push_back(MaxJob{V, B.n, 1, B.s, B.n, st->maxabs + st->gexp[b], 0});
+    const int nkb = B.n / kOzKBlock;
+    sj.push_back(SliceJob{V, B.n, 1, B.s, B.n, st->nw[b], st->ntn[b], 0, nkb,
+                          st->bytes + st->vb_off[b], (long long)nkb * oz_bblock(st->nw[b]),
+                          st->maxabs + st->gexp[b], st->exps + st->gexp[b], 0});
   }
-  ozaki_slice(jobs, s);
+  for (const SliceJob &j : sj) check_slice(j, st->bytes, bytes);
+  const long long mi = ozaki_prepare_max(mj), si = ozaki_prepare_slice(sj);
+  MaxJob *dmj = upload(mj, s);
+  SliceJob *dsj = upload(sj, s);
+  ozaki_max(dmj, (int)mj.size(), mi, nullptr, s);
+  ozaki_slice(dsj, (int)sj.size(), si, nullptr, s);
   HB_CUDA(cudaStreamSynchronize(s));
+  cudaFree(dmj);
+  cudaFree(dsj);
   t.mixed = st;
   return *st;
 }
 
-int covering(int h, int i, int d) {
-  const int j = i >> (h - d);
-  const bool top = ((i >> (h - d - 1)) & 1) == 0;
-  return block_index(d, j, top ? 1 : 2);
-}
-
-MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldy, cudaStream_t s) {
-  auto it = st.plans.find({k, ldy});
+MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long long ldy,
+                      cudaStream_t s) {
+  auto key = std::make_tuple(k, ldx, ldy);
+  auto it = st.plans.find(key);
   if (it != st.plans.end()) return *it->second;
   const Geometry &g = t.g;
-  const int S = kOzSlices, n = g.n, nb = g.nblock(), nl = g.nleaf(), h = g.h;
-  const int npad = pad32(n);
+  const int n = g.n, nb = g.nblock(), nl = g.nleaf(), h = g.h;
+  const int nkbn = n / kOzKBlock;
   auto plan = std::make_unique<MixedPlan>();
   MixedPlan &P = *plan;
   P.k = k;
-  const long long xslice = (long long)k * npad;
-  HB_CUDA(cudaMalloc((void **)&P.xs, std::max<long long>(S * xslice, 16)));
-  HB_CUDA(cudaMalloc((void **)&P.xe, sizeof(int) * std::max(k, 1)));
-  long long wd = 0, wb = 0, we = 0;
-  P.w_off.resize(nb);
-  P.ws_off.resize(nb);
-  P.we_off.resize(nb);
-  for (int b = 0; b < nb; ++b) {
-    const BlockDesc &B = g.blocks[b];
-    P.w_off[b] = wd;
-    wd += align_up((long long)B.s * k);
-    P.ws_off[b] = wb;
-    wb += pad16((long long)S * k * st.spad[b]);
-    P.we_off[b] = we;
-    we += k;
-  }
-  HB_CUDA(cudaMalloc((void **)&P.w, sizeof(double) * std::max<long long>(wd, 1)));
-  HB_CUDA(cudaMalloc((void **)&P.ws, std::max<long long>(wb, 16)));
-  HB_CUDA(cudaMemsetAsync(P.ws, 0, std::max<long long>(wb, 16), s));
-  HB_CUDA(cudaMalloc((void **)&P.we, sizeof(int) * std::max<long long>(we, 1)));
-  HB_CUDA(cudaMalloc((void **)&P.status, sizeof(int)));
+  P.nw2 = std::min(kOzMaxNw, pad16(k));
+  const int nja = (int)cdiv(k, kOzRowsA), njb = (int)cdiv(k, P.nw2);
+  P.xmax = dalloc<unsigned long long>(k);
+  P.fmax = dalloc<unsigned long long>(k);
+  P.xexp = dalloc<int>(k);
+  P.fexp = dalloc<int>(k);
+  const long long xa_size = (long long)nja * nkbn * kOzABlock;
+  const long long xb_size = (long long)njb * nkbn * oz_bblock(P.nw2);
+  P.xa = dalloc<uint8_t>(xa_size);
+  P.xb = dalloc<uint8_t>(xb_size);
+  P.status = dalloc<int>(1);
   HB_CUDA(cudaMemsetAsync(P.status, 0, sizeof(int), s));
+
+  // ---- phase 1 tiles: split long blocks along K so the work spreads -------------
+  long long work = 0;
+  for (int b = 0; b < nb; ++b)
+    if (g.blocks[b].s) work += (long long)st.ntn[b] * st.nw[b] * (g.blocks[b].n / kOzKBlock);
+  work *= nja;
+  const long long target = std::max<long long>(work / (3LL * num_sms()), 64LL * 16);
+  std::vector<int> nch(nb, 1);
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
-    if (B.s == 0) continue;
-    P.wjobs.push_back(SliceJob{P.w + P.w_off[b], B.s, B.s, k, P.ws + P.ws_off[b],
-                               (long long)k * st.spad[b], st.spad[b], P.we + P.we_off[b], 0});
+    if (!B.s) continue;
+    const int nkb = B.n / kOzKBlock;
+    nch[b] = (int)std::max(1LL, std::min<long long>(nkb / 8, cdiv((long long)st.nw[b] * nkb, target)));
+    nch[b] = (int)std::max<long long>(nch[b], cdiv(nkb, kOzMaxK / kOzKBlock));
   }
-  // phase 1 tiles
+  // W^T per block (k x s_b, ld k); blocks split along K first so one memset zeroes them
+  std::vector<long long> w_off(nb, 0);
+  long long wd = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int b = 0; b < nb; ++b) {
+      const BlockDesc &B = g.blocks[b];
+      if (!B.s || (nch[b] > 1) != (pass == 0)) continue;
+      w_off[b] = wd;
+      wd += align_up((long long)B.s * k);
+      if (pass == 0) P.w_zero = wd;
+    }
+  P.w = dalloc<double>(wd);
   std::vector<OzSeg> s1;
   std::vector<OzTile> t1;
-  const int kchunk_max = 2048;
+  std::vector<long long> work1;
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
-    if (B.s == 0) continue;
-    const int nchunks = std::max(1, (B.n + kchunk_max - 1) / kchunk_max);
-    const int chunk = pad32((B.n + nchunks - 1) / nchunks);
-    for (int m0 = 0; m0 < B.s; m0 += kOzM)
-      for (int n0 = 0; n0 < k; n0 += kOzN)
-        for (int k0 = 0; k0 < B.n; k0 += chunk) {
-          OzSeg sg;
-          sg.a = OzOperand{st.bytes + st.v_off[b] + (long long)m0 * pad32(B.n) + k0,
-                           (long long)B.s * pad32(B.n), pad32(B.n), st.exps + st.v_exp[b] + m0};
-          sg.b = OzOperand{P.xs + (long long)n0 * npad + B.c0 + k0, xslice, npad, P.xe + n0};
-          sg.K = std::min(chunk, B.n - k0);
+    if (!B.s) continue;
+    const int nkb = B.n / kOzKBlock, nw = st.nw[b];
+    const int per = (int)cdiv(nkb, nch[b]);
+    for (int tn = 0; tn < st.ntn[b]; ++tn)
+      for (int kb0 = 0; kb0 < nkb; kb0 += per)
+        for (int ja = 0; ja < nja; ++ja) {
+          const int len = std::min(per, nkb - kb0);
+          OzSeg sg{P.xa + ((long long)ja * nkbn + B.c0 / kOzKBlock + kb0) * kOzABlock,
+                   st.bytes + st.vb_off[b] + ((long long)tn * nkb + kb0) * oz_bblock(nw), len, 0};
           OzTile tl;
           tl.seg0 = (int)s1.size();
           tl.nseg = 1;
-          tl.rows = std::min(kOzM, B.s - m0);
-          tl.cols = std::min(kOzN, k - n0);
-          tl.c_off = P.w_off[b] + m0 + (long long)n0 * B.s;
-          tl.ldc = B.s;
-          tl.atomic = 1;
+          tl.rows = std::min(kOzRowsA, k - ja * kOzRowsA);
+          tl.cols = std::min(nw, B.s - tn * nw);
+          tl.nw = nw;
+          tl.atomic = nch[b] > 1;
+          tl.c_off = w_off[b] + ja * kOzRowsA + (long long)tn * nw * k;
+          tl.ldc = k;
+          tl.rexp = P.xexp + ja * kOzRowsA;
+          tl.cexp = st.exps + st.gexp[b] + tn * nw;
           s1.push_back(sg);
           t1.push_back(tl);
+          work1.push_back((long long)len * nw);
         }
   }
-  std::stable_sort(t1.begin(), t1.end(), [&](const OzTile &a, const OzTile &b) {
-    return s1[a.seg0].K > s1[b.seg0].K;
-  });
-  // phase 2 tiles
+  // longest tiles first (round-robin over the persistent grid)
+  std::vector<int> order(t1.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return work1[a] > work1[b]; });
+  std::vector<OzTile> t1s;
+  for (int i : order) t1s.push_back(t1[i]);
+
+  // ---- phase 2 tiles: band-major so a band's column tiles run together ----------
+  std::vector<long long> wb_off(nb, 0);
+  long long wbb = 0;
+  for (int b = 0; b < nb; ++b) {
+    const BlockDesc &B = g.blocks[b];
+    if (!B.s) continue;
+    wb_off[b] = wbb;
+    wbb += (long long)njb * (pad32(B.s) / kOzKBlock) * oz_bblock(P.nw2);
+  }
+  P.wb = dalloc<uint8_t>(wbb);
   std::vector<OzSeg> s2;
   std::vector<OzTile> t2;
   for (int i = 0; i < nl; ++i) {
     const LeafDesc &L = t.leaves[i];
-    for (int m0 = 0; m0 < L.m; m0 += kOzM)
-      for (int n0 = 0; n0 < k; n0 += kOzN) {
+    const long long stride = (long long)st.band_nkb[i] * kOzABlock;
+    for (int m0 = 0, band = 0; m0 < L.m; m0 += kOzRowsA, ++band)
+      for (int jb = 0; jb < njb; ++jb) {
         OzTile tl;
         tl.seg0 = (int)s2.size();
         tl.nseg = 0;
-        tl.rows = std::min(kOzM, L.m - m0);
-        tl.cols = std::min(kOzN, k - n0);
-        tl.c_off = L.r0 + m0 + (long long)n0 * ldy;
-        tl.ldc = ldy;
+        tl.rows = std::min(kOzRowsA, L.m - m0);
+        tl.cols = std::min(P.nw2, k - jb * P.nw2);
+        tl.nw = P.nw2;
         tl.atomic = 0;
-        OzSeg sd;
-        sd.a = OzOperand{st.bytes + st.d_off[i] + (long long)m0 * st.kpad[i],
-                         (long long)L.m * st.kpad[i], st.kpad[i], st.exps + st.d_exp[i] + m0};
-        sd.b = OzOperand{P.xs + (long long)n0 * npad + L.r0, xslice, npad, P.xe + n0};
-        sd.K = st.kpad[i];
-        s2.push_back(sd);
+        tl.c_off = L.r0 + m0 + (long long)jb * P.nw2 * ldy;
+        tl.ldc = ldy;
+        tl.rexp = st.exps + L.r0 + m0;
+        tl.cexp = P.fexp + jb * P.nw2;
+        const uint8_t *a = st.bytes + st.band_off[i] + band * stride;
+        const int nkd = L.m / kOzKBlock;
+        s2.push_back(OzSeg{a, P.xb + ((long long)jb * nkbn + L.r0 / kOzKBlock) * oz_bblock(P.nw2),
+                           nkd, 0});
+        a += (long long)nkd * kOzABlock;
         ++tl.nseg;
         for (int d = h - 1; d >= 0; --d) {
           const int b = covering(h, i, d);
           const BlockDesc &B = g.blocks[b];
-          if (B.s == 0) continue;
-          const int roff = L.r0 + m0 - B.r0;
-          OzSeg su;
-          su.a = OzOperand{st.bytes + st.u_off[b] + (long long)roff * st.spad[b],
-                           (long long)B.m * st.spad[b], st.spad[b], st.exps + st.u_exp[b] + roff};
-          su.b = OzOperand{P.ws + P.ws_off[b] + (long long)n0 * st.spad[b],
-                           (long long)k * st.spad[b], st.spad[b], P.we + P.we_off[b] + n0};
-          su.K = st.spad[b];
-          s2.push_back(su);
+          if (!B.s) continue;
+          const int nks = pad32(B.s) / kOzKBlock;
+          s2.push_back(
+              OzSeg{a, P.wb + wb_off[b] + (long long)jb * nks * oz_bblock(P.nw2), nks, 0});
+          a += (long long)nks * kOzABlock;
           ++tl.nseg;
         }
         t2.push_back(tl);
       }
   }
+
+  // ---- exponent and slicing jobs --------------------------------------------------
+  std::vector<MaxJob> mx{MaxJob{nullptr, ldx, 1, k, n, P.xmax, 0}};
+  std::vector<MaxJob> mw;
+  std::vector<SliceJob> sx{SliceJob{nullptr, ldx, 1, k, n, kOzRowsA, nja, 0, nkbn, P.xa,
+                                    (long long)nkbn * kOzABlock, P.xmax, P.xexp, 0}};
+  std::vector<SliceJob> sb{SliceJob{nullptr, ldx, 1, k, n, P.nw2, njb, 0, nkbn, P.xb,
+                                    (long long)nkbn * oz_bblock(P.nw2), P.fmax, P.fexp, 0}};
+  for (int b = 0; b < nb; ++b) {
+    const BlockDesc &B = g.blocks[b];
+    if (!B.s) continue;
+    const double *wt = P.w + w_off[b];
+    mw.push_back(MaxJob{wt, 1, k, k, B.s, P.fmax, 0});
+    const int nks = pad32(B.s) / kOzKBlock;
+    sb.push_back(SliceJob{wt, 1, k, k, B.s, P.nw2, njb, 0, nks, P.wb + wb_off[b],
+                          (long long)nks * oz_bblock(P.nw2), P.fmax, nullptr, 0});
+  }
+  for (size_t i = 0; i < t1.size(); ++i) {
+    const OzTile &tl = t1[i];
+    check_seg(s1[tl.seg0], tl.nw, P.xa, xa_size, st.bytes, st.nbytes, nullptr, 0);
+    HB_REQUIRE(tl.c_off >= 0 && tl.c_off + (tl.rows - 1) + (tl.cols - 1) * tl.ldc < wd,
+               INPUT_ERROR, "mixed plan: phase-1 tile outside W");
+  }
+  for (const OzTile &tl : t2) {
+    long long K = 0;
+    for (int q = tl.seg0; q < tl.seg0 + tl.nseg; ++q) {
+      check_seg(s2[q], tl.nw, st.bytes, st.nbytes, P.xb, xb_size, P.wb, wbb);
+      K += (long long)s2[q].nkb * kOzKBlock;
+    }
+    HB_REQUIRE(K <= kOzMaxK, INPUT_ERROR, "mixed plan: tile K above 65536");
+  }
+  check_slice(sx[0], P.xa, xa_size);
+  check_slice(sb[0], P.xb, xb_size);
+  for (size_t i = 1; i < sb.size(); ++i) check_slice(sb[i], P.wb, wbb);
+  P.it_max_x = ozaki_prepare_max(mx);
+  P.it_max_w = ozaki_prepare_max(mw);
+  P.it_sl_x = ozaki_prepare_slice(sx);
+  P.it_sl_b = ozaki_prepare_slice(sb);
+  P.n_max_w = (int)mw.size();
+  P.n_sl_b = (int)sb.size();
+  P.max_x = upload(mx, s);
+  P.max_w = upload(mw, s);
+  P.sl_x = upload(sx, s);
+  P.sl_b = upload(sb, s);
   P.seg1 = upload(s1, s);
-  P.tile1 = upload(t1, s);
-  P.ntile1 = (int)t1.size();
+  P.tile1 = upload(t1s, s);
+  P.ntile1 = (int)t1s.size();
   P.seg2 = upload(s2, s);
   P.tile2 = upload(t2, s);
   P.ntile2 = (int)t2.size();
   HB_CUDA(cudaStreamSynchronize(s));
   auto &ref = *plan;
-  st.plans[{k, ldy}] = std::move(plan);
+  st.plans[key] = std::move(plan);
   return ref;
 }
 
@@ -261,21 +409,23 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldy, cudaS
 void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double *Y, long long ldy,
                    cudaStream_t s) {
   if (k <= 0 || t.g.n == 0) return;
+  HB_REQUIRE(ldx >= t.g.n && ldy >= t.g.n, INPUT_ERROR, "leading dimension below n");
   std::lock_guard<std::mutex> lk(t.plan_mutex);
   MixedState &st = mixed_state(t, s);
-  MixedPlan &P = mixed_plan(t, st, k, ldy, s);
-  const int n = t.g.n, npad = pad32(n);
+  MixedPlan &P = mixed_plan(t, st, k, ldx, ldy, s);
   PhaseTimer timer(s);
-  // 1. slice X (columns, over all rows)
-  ozaki_slice({SliceJob{X, ldx, n, k, P.xs, (long long)k * npad, npad, P.xe, 0}}, s);
-  // 2. W = V^T X (split K, atomics into zeroed W)
-  long long wtot = 0;
-  for (auto &B : t.g.blocks) wtot += align_up((long long)B.s * k);
-  HB_CUDA(cudaMemsetAsync(P.w, 0, sizeof(double) * std::max<long long>(wtot, 1), s));
+  // 1. exponents and slices of X for phase 1; W^T = X^T V per block
+  HB_CUDA(cudaMemsetAsync(P.xmax, 0, sizeof(unsigned long long) * k, s));
+  ozaki_max(P.max_x, 1, P.it_max_x, X, s);
+  ozaki_slice(P.sl_x, 1, P.it_sl_x, X, s);
+  if (P.w_zero) HB_CUDA(cudaMemsetAsync(P.w, 0, sizeof(double) * P.w_zero, s));
   ozaki_gemm(P.seg1, P.tile1, P.ntile1, P.w, P.status, s);
   timer.mark(1);
-  // 3. slice W per block; 4. Y = D X + sum U W
-  ozaki_slice(P.wjobs, s);
+  // 2. common column exponents of X and W, their slices; Y band by band
+  HB_CUDA(cudaMemcpyAsync(P.fmax, P.xmax, sizeof(unsigned long long) * k,
+                          cudaMemcpyDeviceToDevice, s));
+  ozaki_max(P.max_w, P.n_max_w, P.it_max_w, X, s);
+  ozaki_slice(P.sl_b, P.n_sl_b, P.it_sl_b, X, s);
   ozaki_gemm(P.seg2, P.tile2, P.ntile2, Y, P.status, s);
   timer.mark(2);
 }

@@ -66,6 +66,30 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return false;
 }
 
+// Arrive once on `bar` and add `bytes` to the transaction count its current
+// phase waits for (the bulk copies issued against it complete the bytes).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// ---- bulk copy ------------------------------------------------------------------
+// Contiguous global -> shared copy by the async proxy (16-byte aligned
+// addresses, size a multiple of 16); completes `bytes` on `bar`.  The
+// destination is this CTA's own shared memory.
+__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
+          "r"(smem_u32(smem_dst)),
+      "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // ---- descriptors -----------------------------------------------------------------
 // Shared-memory matrix descriptor (sm_100): start address >> 4 in bits 0-13,
 // leading-dimension byte offset >> 4 in 16-29, stride-dimension byte offset
