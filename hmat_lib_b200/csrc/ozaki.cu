@@ -56,6 +56,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
   __shared__ __align__(8) uint64_t tmem_full, tmem_empty, mma_done;
   __shared__ uint32_t taddr_s;
   __shared__ volatile int bad;
+  __shared__ int cexp_s[4][kOzMaxNw];   // per epilogue warp: column exponents of its tile
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 1) {
@@ -165,6 +166,10 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++lt) {
       if (__any_sync(0xffffffffu, bad)) break;
       const OzTile T = tiles[tile];
+      // column exponents of this tile, staged while its MMAs run
+      __syncwarp();
+      for (int j = lane; j < kOzMaxNw; j += 32) cexp_s[quarter][j] = j < T.cols ? T.cexp[j] : 0;
+      __syncwarp();
       const bool ready = wait_or_abort(&tmem_full, (uint32_t)(lt & 1), &bad);
       if (!__all_sync(0xffffffffu, ready)) {
         bad = 1;
@@ -173,8 +178,9 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       umma::fence_after_sync();
       const int nw = T.nw;
       const bool row_ok = r < T.rows;
-      const int er = row_ok ? T.rexp[r] : 0;
+      const int er = (row_ok ? T.rexp[r] : 0) - 14;
       double *crow = cbase + T.c_off + r;
+      double rowmax = 0.0;
       for (int c0 = 0; c0 < nw; c0 += 16) {
         int32_t v[kOzSlices][16];
 #pragma unroll
@@ -189,7 +195,11 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
             double acc = (double)v[kOzSlices - 1][x];
 #pragma unroll
             for (int t = kOzSlices - 2; t >= 0; --t) acc = fma(acc, 0x1p-7, (double)v[t][x]);
-            const double val = ldexp(acc, er + T.cexp[j] - 14);
+            const int e = er + cexp_s[quarter][j];
+            const double val = (e >= -1022 && e <= 1023)
+                                   ? acc * __longlong_as_double((long long)(e + 1023) << 52)
+                                   : ldexp(acc, e);
+            rowmax = fmax(rowmax, fabs(val));
             double *c = crow + (long long)j * T.ldc;
             if (T.atomic)
               atomicAdd(c, val);
@@ -198,6 +208,8 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
           }
         }
       }
+      if (T.rmax && row_ok && rowmax > 0.0)
+        atomicMax(T.rmax + r, (unsigned long long)__double_as_longlong(rowmax));
       umma::fence_before_sync();
       __syncwarp();
       if (lane == 0) umma::mbar_arrive(&tmem_empty);
@@ -237,42 +249,93 @@ __device__ __forceinline__ int find_job(const Job *jobs, int njobs, long long it
   return lo;
 }
 
-// Work items are warps: a line (K contiguous: lanes split K) or 32 lines (one
-// per lane, loop over K).
+constexpr int kMaxChunkK = 2048;   // K values per warp item, K-contiguous lines
+constexpr int kMaxChunkL = 64;     // K values per warp item, line-contiguous (32 lines)
+constexpr int kTileLines = 32;     // shared-memory transpose tile: lines x K values
+constexpr int kTileK = 128;
+
+__device__ __forceinline__ void max_into(unsigned long long *out, double mx) {
+  if (mx > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
+}
+
+// Work items are warps: one line and kMaxChunkK of its K values (K
+// contiguous: lanes split K), or 32 lines (one per lane) and kMaxChunkL K
+// values.
 __global__ void max_kernel(const MaxJob *__restrict__ jobs, int njobs, long long items,
                            const double *xbase) {
   const int lane = threadIdx.x & 31;
   const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long it = w0; it < items; it += nw) {
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long it = w0; it < items; it += nwarps) {
     const MaxJob &J = jobs[find_job(jobs, njobs, it)];
     const double *src = J.src ? J.src : xbase;
     const long long local = it - J.item0;
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
     if (J.s_k == 1) {
-      const double *row = src + local * J.s_line;
-      double mx = 0.0;
-      for (int k = lane; k < J.K; k += 32) mx = fmax(mx, fabs(row[k]));
+      const int nch = (J.K + kMaxChunkK - 1) / kMaxChunkK;
+      const long long line = local / nch;
+      const int k0 = (int)(local % nch) * kMaxChunkK, k1 = min(J.K, k0 + kMaxChunkK);
+      const double *row = src + line * J.s_line;
+      int k = k0 + lane;
+      for (; k + 96 < k1; k += 128) {
+        m0 = fmax(m0, fabs(row[k]));
+        m1 = fmax(m1, fabs(row[k + 32]));
+        m2 = fmax(m2, fabs(row[k + 64]));
+        m3 = fmax(m3, fabs(row[k + 96]));
+      }
+      for (; k < k1; k += 32) m0 = fmax(m0, fabs(row[k]));
+      double mx = fmax(fmax(m0, m1), fmax(m2, m3));
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      if (lane == 0 && mx > 0.0)
-        atomicMax(J.out + local, (unsigned long long)__double_as_longlong(mx));
+      if (lane == 0) max_into(J.out + line, mx);
     } else {
-      const long long line = local * 32 + lane;
+      const int nch = (J.K + kMaxChunkL - 1) / kMaxChunkL;
+      const long long line = (local / nch) * 32 + lane;
+      const int k0 = (int)(local % nch) * kMaxChunkL, k1 = min(J.K, k0 + kMaxChunkL);
       if (line < J.lines) {
-        double mx = 0.0;
         const double *p = src + line * J.s_line;
-        for (int k = 0; k < J.K; ++k) mx = fmax(mx, fabs(p[(long long)k * J.s_k]));
-        if (mx > 0.0) atomicMax(J.out + line, (unsigned long long)__double_as_longlong(mx));
+        int k = k0;
+        for (; k + 3 < k1; k += 4) {
+          m0 = fmax(m0, fabs(p[(long long)k * J.s_k]));
+          m1 = fmax(m1, fabs(p[(long long)(k + 1) * J.s_k]));
+          m2 = fmax(m2, fabs(p[(long long)(k + 2) * J.s_k]));
+          m3 = fmax(m3, fabs(p[(long long)(k + 3) * J.s_k]));
+        }
+        for (; k < k1; ++k) m0 = fmax(m0, fabs(p[(long long)k * J.s_k]));
+        max_into(J.out + line, fmax(fmax(m0, m1), fmax(m2, m3)));
       }
     }
   }
 }
 
-// One item = 16 consecutive K positions of one line: six aligned 16-byte
-// stores, one per slice.  Lines vary fastest, so eight neighbouring items
-// fill one 128-byte core matrix.
-__global__ void slice_kernel(const SliceJob *__restrict__ jobs, int njobs, long long items,
-                             const double *xbase) {
+// Six slices of 16 consecutive K values of one line, scaled by 2^-ex, stored
+// as six aligned 16-byte words at `base` + p R 32.
+__device__ __forceinline__ void slice16(const double (&y0)[16], int ex, uint8_t *base, int R) {
+  int8_t out[kOzSlices][16];
+#pragma unroll
+  for (int x = 0; x < 16; ++x) {
+    double y = ldexp(y0[x], -ex);
+#pragma unroll
+    for (int p = 0; p < kOzSlices; ++p) {
+      y *= 128.0;
+      const double a = rint(y);
+      out[p][x] = (int8_t)a;
+      y -= a;
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < kOzSlices; ++p) {
+    int4 w;
+    memcpy(&w, out[p], 16);
+    *reinterpret_cast<int4 *>(base + (long long)p * R * kOzKBlock) = w;
+  }
+}
+
+// Line-contiguous sources: one item = 16 consecutive K positions of one
+// line; lines vary fastest, so loads are coalesced and eight neighbouring
+// items fill one 128-byte core matrix.
+__global__ void slice_lines_kernel(const SliceJob *__restrict__ jobs, int njobs, long long items,
+                                   const double *xbase) {
   for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < items;
        it += (long long)gridDim.x * blockDim.x) {
     const SliceJob &J = jobs[find_job(jobs, njobs, it)];
@@ -283,29 +346,53 @@ __global__ void slice_kernel(const SliceJob *__restrict__ jobs, int njobs, long 
     const bool live = line < J.lines;
     const int ex = live ? scale_exponent(J.maxabs[line]) : 0;
     if (J.exp_out && c16 == 0 && live) J.exp_out[line] = ex;
-    int8_t out[kOzSlices][16];
+    double y[16];
 #pragma unroll
     for (int x = 0; x < 16; ++x) {
       const int k = c16 * 16 + x;
-      double y = (live && k < J.K) ? src[(long long)line * J.s_line + (long long)k * J.s_k] : 0.0;
-      y = ldexp(y, -ex);
-#pragma unroll
-      for (int p = 0; p < kOzSlices; ++p) {
-        y *= 128.0;
-        const double a = rint(y);
-        out[p][x] = (int8_t)a;
-        y -= a;
-      }
+      y[x] = (live && k < J.K) ? src[(long long)line * J.s_line + (long long)k * J.s_k] : 0.0;
     }
     const int t = line / J.R, lr = line % J.R;
-    uint8_t *base = J.dst + (long long)t * J.tile_stride +
-                    oz_offset(J.R, 0, lr, (J.kb0 * kOzKBlock) + c16 * 16);
-#pragma unroll
-    for (int p = 0; p < kOzSlices; ++p) {
-      int4 w;
-      memcpy(&w, out[p], 16);
-      *reinterpret_cast<int4 *>(base + (long long)p * J.R * kOzKBlock) = w;
+    slice16(y, ex, J.dst + (long long)t * J.tile_stride +
+                       oz_offset(J.R, 0, lr, J.kb0 * kOzKBlock + c16 * 16), J.R);
+  }
+}
+
+// K-contiguous sources (s_k = 1): one block item = 32 lines x 128 K values,
+// read with coalesced row loads into shared memory, then sliced 16 K values
+// per thread.
+__global__ void __launch_bounds__(256) slice_kcontig_kernel(const SliceJob *__restrict__ jobs,
+                                                            int njobs, long long items,
+                                                            const double *xbase) {
+  __shared__ double buf[kTileLines][kTileK + 1];
+  const int tid = threadIdx.x;
+  for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    const SliceJob &J = jobs[find_job(jobs, njobs, it)];
+    const double *src = J.src ? J.src : xbase;
+    const long long local = it - J.item0;
+    const int Kw = J.nkb * kOzKBlock;                   // K positions written
+    const int nkt = (Kw + kTileK - 1) / kTileK;
+    const int line0 = (int)(local / nkt) * kTileLines, k0 = (int)(local % nkt) * kTileK;
+    for (int idx = tid; idx < kTileLines * kTileK; idx += blockDim.x) {
+      const int l = idx / kTileK, kk = idx % kTileK;
+      const int line = line0 + l, k = k0 + kk;
+      buf[l][kk] = (line < J.lines && k < J.K) ? src[(long long)line * J.s_line + k] : 0.0;
     }
+    __syncthreads();
+    const int l = tid % kTileLines, c = tid / kTileLines;   // 8 chunks of 16
+    const int line = line0 + l, k = k0 + c * 16;
+    if (line < J.ntiles * J.R && k < Kw) {
+      const bool live = line < J.lines;
+      const int ex = live ? scale_exponent(J.maxabs[line]) : 0;
+      if (J.exp_out && k == 0 && live) J.exp_out[line] = ex;
+      double y[16];
+#pragma unroll
+      for (int x = 0; x < 16; ++x) y[x] = buf[l][c * 16 + x];
+      const int t = line / J.R, lr = line % J.R;
+      slice16(y, ex, J.dst + (long long)t * J.tile_stride +
+                         oz_offset(J.R, 0, lr, J.kb0 * kOzKBlock + k), J.R);
+    }
+    __syncthreads();
   }
 }
 
@@ -330,36 +417,57 @@ void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *
   HB_LAUNCHED();
 }
 
-long long ozaki_prepare_max(std::vector<MaxJob> &jobs) {
-  long long items = 0;
+MaxBatch ozaki_max_batch(std::vector<MaxJob> jobs, cudaStream_t stream) {
+  MaxBatch b;
   for (auto &j : jobs) {
-    j.item0 = items;
-    items += (j.s_k == 1) ? j.lines : (j.lines + 31) / 32;
+    j.item0 = b.items;
+    b.items += (j.s_k == 1) ? (long long)j.lines * ((j.K + kMaxChunkK - 1) / kMaxChunkK)
+                            : (long long)((j.lines + 31) / 32) * ((j.K + kMaxChunkL - 1) / kMaxChunkL);
   }
-  return items;
+  b.n = (int)jobs.size();
+  if (b.n) {
+    HB_CUDA(cudaMalloc((void **)&b.d, sizeof(MaxJob) * jobs.size()));
+    HB_CUDA(cudaMemcpyAsync(b.d, jobs.data(), sizeof(MaxJob) * jobs.size(), cudaMemcpyHostToDevice,
+                            stream));
+  }
+  return b;
 }
 
-long long ozaki_prepare_slice(std::vector<SliceJob> &jobs) {
-  long long items = 0;
+SliceBatch ozaki_slice_batch(std::vector<SliceJob> jobs, cudaStream_t stream) {
+  SliceBatch b;
+  b.kcontig = !jobs.empty() && jobs[0].s_k == 1;
   for (auto &j : jobs) {
     HB_REQUIRE(j.R % 8 == 0 && j.R >= 8, INPUT_ERROR, "slice tile lines");
-    j.item0 = items;
-    items += (long long)j.ntiles * j.R * j.nkb * 2;
+    HB_REQUIRE((j.s_k == 1) == b.kcontig, INPUT_ERROR, "mixed slice job kinds in one batch");
+    j.item0 = b.items;
+    const long long L = (long long)j.ntiles * j.R;
+    b.items += b.kcontig ? ((L + kTileLines - 1) / kTileLines) *
+                               ((j.nkb * kOzKBlock + kTileK - 1) / kTileK)
+                         : L * j.nkb * 2;
   }
-  return items;
+  b.n = (int)jobs.size();
+  if (b.n) {
+    HB_CUDA(cudaMalloc((void **)&b.d, sizeof(SliceJob) * jobs.size()));
+    HB_CUDA(cudaMemcpyAsync(b.d, jobs.data(), sizeof(SliceJob) * jobs.size(),
+                            cudaMemcpyHostToDevice, stream));
+  }
+  return b;
 }
 
-void ozaki_max(const MaxJob *d_jobs, int njobs, long long items, const double *xbase,
-               cudaStream_t stream) {
-  if (njobs <= 0 || items <= 0) return;
-  max_kernel<<<grid_for(items * 32), 256, 0, stream>>>(d_jobs, njobs, items, xbase);
+void ozaki_max(const MaxBatch &b, const double *xbase, cudaStream_t stream) {
+  if (b.n <= 0 || b.items <= 0) return;
+  max_kernel<<<grid_for(b.items * 32), 256, 0, stream>>>(b.d, b.n, b.items, xbase);
   HB_LAUNCHED();
 }
 
-void ozaki_slice(const SliceJob *d_jobs, int njobs, long long items, const double *xbase,
-                 cudaStream_t stream) {
-  if (njobs <= 0 || items <= 0) return;
-  slice_kernel<<<grid_for(items), 256, 0, stream>>>(d_jobs, njobs, items, xbase);
+void ozaki_slice(const SliceBatch &b, const double *xbase, cudaStream_t stream) {
+  if (b.n <= 0 || b.items <= 0) return;
+  if (b.kcontig) {
+    const int grid = (int)std::min<long long>(b.items, (long long)num_sms() * 8);
+    slice_kcontig_kernel<<<grid, 256, 0, stream>>>(b.d, b.n, b.items, xbase);
+  } else {
+    slice_lines_kernel<<<grid_for(b.items), 256, 0, stream>>>(b.d, b.n, b.items, xbase);
+  }
   HB_LAUNCHED();
 }
 

@@ -59,6 +59,8 @@ struct OzSeg {
 // One 128 x nw output tile: the K segments seg0 .. seg0 + nseg - 1 all share
 // the row exponents rexp[0 .. rows) and column exponents cexp[0 .. cols), so
 // the tile is recombined once.  Element (r, j) goes to cbase[c_off + r + j ldc].
+// rmax, if set, receives (atomic max, double bits) the largest |result| of
+// every row of the tile.
 struct OzTile {
   int seg0, nseg;
   int rows, cols;
@@ -66,6 +68,7 @@ struct OzTile {
   int atomic;      // 1: add atomically (K split over several tiles)
   long long c_off, ldc;
   const int *rexp, *cexp;
+  unsigned long long *rmax;
 };
 
 // Runs all tiles with a persistent grid (one CTA per SM).  `status` (device
@@ -77,7 +80,7 @@ void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *
 // src[line * s_line + k * s_k], combined by atomic max into out[line] (the
 // bit pattern of a non-negative double; zero it first).  A NULL src stands
 // for the `xbase` argument of the launch.  item0: prefix over the jobs of
-// their work items (filled by ozaki_prepare_max).
+// their work items (filled when the batch is made).
 struct MaxJob {
   const double *src;
   long long s_line, s_k;
@@ -102,12 +105,22 @@ struct SliceJob {
   long long item0;
 };
 
-// Fill item0 and return the total item count.
-long long ozaki_prepare_max(std::vector<MaxJob> &jobs);
-long long ozaki_prepare_slice(std::vector<SliceJob> &jobs);
-void ozaki_max(const MaxJob *d_jobs, int njobs, long long items, const double *xbase,
-               cudaStream_t stream);
-void ozaki_slice(const SliceJob *d_jobs, int njobs, long long items, const double *xbase,
-                 cudaStream_t stream);
+// Job lists uploaded once.  A slice batch is either all K-contiguous (s_k = 1:
+// read through a shared-memory transpose) or all line-contiguous.
+struct MaxBatch {
+  MaxJob *d = nullptr;
+  int n = 0;
+  long long items = 0;
+};
+struct SliceBatch {
+  SliceJob *d = nullptr;
+  int n = 0;
+  long long items = 0;
+  bool kcontig = false;
+};
+MaxBatch ozaki_max_batch(std::vector<MaxJob> jobs, cudaStream_t stream);
+SliceBatch ozaki_slice_batch(std::vector<SliceJob> jobs, cudaStream_t stream);
+void ozaki_max(const MaxBatch &b, const double *xbase, cudaStream_t stream);
+void ozaki_slice(const SliceBatch &b, const double *xbase, cudaStream_t stream);
 
 }  // namespace hb

@@ -103,18 +103,17 @@ struct MixedPlan {
   uint8_t *xa = nullptr, *xb = nullptr, *wb = nullptr;
   double *w = nullptr;
   long long w_zero = 0;                    // leading doubles of w added to atomically
-  MaxJob *max_x = nullptr, *max_w = nullptr;
-  SliceJob *sl_x = nullptr, *sl_b = nullptr;
-  int n_max_w = 0, n_sl_b = 0;
-  long long it_max_x = 0, it_max_w = 0, it_sl_x = 0, it_sl_b = 0;
+  MaxBatch max_x, max_wsplit;
+  SliceBatch sl_xa, sl_xb, sl_wb;
   OzSeg *seg1 = nullptr, *seg2 = nullptr;
   OzTile *tile1 = nullptr, *tile2 = nullptr;
   int ntile1 = 0, ntile2 = 0;
   int *status = nullptr;
   ~MixedPlan() {
     for (void *p : {(void *)xmax, (void *)fmax, (void *)xexp, (void *)fexp, (void *)xa, (void *)xb,
-                    (void *)wb, (void *)w, (void *)max_x, (void *)max_w, (void *)sl_x, (void *)sl_b,
-                    (void *)seg1, (void *)seg2, (void *)tile1, (void *)tile2, (void *)status})
+                    (void *)wb, (void *)w, (void *)max_x.d, (void *)max_wsplit.d, (void *)sl_xa.d,
+                    (void *)sl_xb.d, (void *)sl_wb.d, (void *)seg1, (void *)seg2, (void *)tile1,
+                    (void *)tile2, (void *)status})
       if (p) cudaFree(p);
   }
 };
@@ -168,7 +167,7 @@ MixedState &mixed_state(DeviceTree &t, cudaStream_t s) {
   HB_CUDA(cudaMemsetAsync(st->maxabs, 0, sizeof(unsigned long long) * nexp, s));
 
   std::vector<MaxJob> mj;
-  std::vector<SliceJob> sj;
+  std::vector<SliceJob> sj, sv;   // line-contiguous (D, U) and K-contiguous (V) sources
   for (int i = 0; i < nl; ++i) {
     const LeafDesc &L = t.leaves[i];
     const int bands = (int)cdiv(L.m, kOzRowsA);
@@ -196,19 +195,20 @@ MixedState &mixed_state(DeviceTree &t, cudaStream_t s) {
     const double *V = t.arena + B.v_off;
     mj.push_back(MaxJob{V, B.n, 1, B.s, B.n, st->maxabs + st->gexp[b], 0});
     const int nkb = B.n / kOzKBlock;
-    sj.push_back(SliceJob{V, B.n, 1, B.s, B.n, st->nw[b], st->ntn[b], 0, nkb,
+    sv.push_back(SliceJob{V, B.n, 1, B.s, B.n, st->nw[b], st->ntn[b], 0, nkb,
                           st->bytes + st->vb_off[b], (long long)nkb * oz_bblock(st->nw[b]),
                           st->maxabs + st->gexp[b], st->exps + st->gexp[b], 0});
   }
   for (const SliceJob &j : sj) check_slice(j, st->bytes, bytes);
-  const long long mi = ozaki_prepare_max(mj), si = ozaki_prepare_slice(sj);
-  MaxJob *dmj = upload(mj, s);
-  SliceJob *dsj = upload(sj, s);
-  ozaki_max(dmj, (int)mj.size(), mi, nullptr, s);
-  ozaki_slice(dsj, (int)sj.size(), si, nullptr, s);
+  for (const SliceJob &j : sv) check_slice(j, st->bytes, bytes);
+  MaxBatch bm = ozaki_max_batch(mj, s);
+  SliceBatch bs = ozaki_slice_batch(sj, s), bv = ozaki_slice_batch(sv, s);
+  ozaki_max(bm, nullptr, s);
+  ozaki_slice(bs, nullptr, s);
+  ozaki_slice(bv, nullptr, s);
   HB_CUDA(cudaStreamSynchronize(s));
-  cudaFree(dmj);
-  cudaFree(dsj);
+  for (void *p : {(void *)bm.d, (void *)bs.d, (void *)bv.d})
+    if (p) cudaFree(p);
   t.mixed = st;
   return *st;
 }
@@ -288,6 +288,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
           tl.ldc = k;
           tl.rexp = P.xexp + ja * kOzRowsA;
           tl.cexp = st.exps + st.gexp[b] + tn * nw;
+          tl.rmax = nch[b] > 1 ? nullptr : P.fmax + ja * kOzRowsA;
           s1.push_back(sg);
           t1.push_back(tl);
           work1.push_back((long long)len * nw);
@@ -329,6 +330,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
         tl.ldc = ldy;
         tl.rexp = st.exps + L.r0 + m0;
         tl.cexp = P.fexp + jb * P.nw2;
+        tl.rmax = nullptr;
         const uint8_t *a = st.bytes + st.band_off[i] + band * stride;
         const int nkd = L.m / kOzKBlock;
         s2.push_back(OzSeg{a, P.xb + ((long long)jb * nkbn + L.r0 / kOzKBlock) * oz_bblock(P.nw2),
@@ -351,16 +353,17 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
 
   // ---- exponent and slicing jobs --------------------------------------------------
   std::vector<MaxJob> mx{MaxJob{nullptr, ldx, 1, k, n, P.xmax, 0}};
-  std::vector<MaxJob> mw;
+  std::vector<MaxJob> mw;   // W of the blocks split along K (the others: phase-1 epilogue)
   std::vector<SliceJob> sx{SliceJob{nullptr, ldx, 1, k, n, kOzRowsA, nja, 0, nkbn, P.xa,
                                     (long long)nkbn * kOzABlock, P.xmax, P.xexp, 0}};
-  std::vector<SliceJob> sb{SliceJob{nullptr, ldx, 1, k, n, P.nw2, njb, 0, nkbn, P.xb,
-                                    (long long)nkbn * oz_bblock(P.nw2), P.fmax, P.fexp, 0}};
+  std::vector<SliceJob> sxb{SliceJob{nullptr, ldx, 1, k, n, P.nw2, njb, 0, nkbn, P.xb,
+                                     (long long)nkbn * oz_bblock(P.nw2), P.fmax, P.fexp, 0}};
+  std::vector<SliceJob> sb;
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
     if (!B.s) continue;
     const double *wt = P.w + w_off[b];
-    mw.push_back(MaxJob{wt, 1, k, k, B.s, P.fmax, 0});
+    if (nch[b] > 1) mw.push_back(MaxJob{wt, 1, k, k, B.s, P.fmax, 0});
     const int nks = pad32(B.s) / kOzKBlock;
     sb.push_back(SliceJob{wt, 1, k, k, B.s, P.nw2, njb, 0, nks, P.wb + wb_off[b],
                           (long long)nks * oz_bblock(P.nw2), P.fmax, nullptr, 0});
@@ -380,18 +383,13 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
     HB_REQUIRE(K <= kOzMaxK, INPUT_ERROR, "mixed plan: tile K above 65536");
   }
   check_slice(sx[0], P.xa, xa_size);
-  check_slice(sb[0], P.xb, xb_size);
-  for (size_t i = 1; i < sb.size(); ++i) check_slice(sb[i], P.wb, wbb);
-  P.it_max_x = ozaki_prepare_max(mx);
-  P.it_max_w = ozaki_prepare_max(mw);
-  P.it_sl_x = ozaki_prepare_slice(sx);
-  P.it_sl_b = ozaki_prepare_slice(sb);
-  P.n_max_w = (int)mw.size();
-  P.n_sl_b = (int)sb.size();
-  P.max_x = upload(mx, s);
-  P.max_w = upload(mw, s);
-  P.sl_x = upload(sx, s);
-  P.sl_b = upload(sb, s);
+  check_slice(sxb[0], P.xb, xb_size);
+  for (const SliceJob &j : sb) check_slice(j, P.wb, wbb);
+  P.max_x = ozaki_max_batch(mx, s);
+  P.max_wsplit = ozaki_max_batch(mw, s);
+  P.sl_xa = ozaki_slice_batch(sx, s);
+  P.sl_xb = ozaki_slice_batch(sxb, s);
+  P.sl_wb = ozaki_slice_batch(sb, s);
   P.seg1 = upload(s1, s);
   P.tile1 = upload(t1s, s);
   P.ntile1 = (int)t1s.size();
@@ -414,18 +412,20 @@ void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double 
   MixedState &st = mixed_state(t, s);
   MixedPlan &P = mixed_plan(t, st, k, ldx, ldy, s);
   PhaseTimer timer(s);
-  // 1. exponents and slices of X for phase 1; W^T = X^T V per block
+  // 1. exponents and slices of X for phase 1; W^T = X^T V per block (the
+  //    epilogue also folds the column maxima of unsplit blocks into fmax)
   HB_CUDA(cudaMemsetAsync(P.xmax, 0, sizeof(unsigned long long) * k, s));
-  ozaki_max(P.max_x, 1, P.it_max_x, X, s);
-  ozaki_slice(P.sl_x, 1, P.it_sl_x, X, s);
+  ozaki_max(P.max_x, X, s);
+  ozaki_slice(P.sl_xa, X, s);
+  HB_CUDA(cudaMemcpyAsync(P.fmax, P.xmax, sizeof(unsigned long long) * k,
+                          cudaMemcpyDeviceToDevice, s));
   if (P.w_zero) HB_CUDA(cudaMemsetAsync(P.w, 0, sizeof(double) * P.w_zero, s));
   ozaki_gemm(P.seg1, P.tile1, P.ntile1, P.w, P.status, s);
   timer.mark(1);
   // 2. common column exponents of X and W, their slices; Y band by band
-  HB_CUDA(cudaMemcpyAsync(P.fmax, P.xmax, sizeof(unsigned long long) * k,
-                          cudaMemcpyDeviceToDevice, s));
-  ozaki_max(P.max_w, P.n_max_w, P.it_max_w, X, s);
-  ozaki_slice(P.sl_b, P.n_sl_b, P.it_sl_b, X, s);
+  ozaki_max(P.max_wsplit, X, s);
+  ozaki_slice(P.sl_xb, X, s);
+  ozaki_slice(P.sl_wb, X, s);
   ozaki_gemm(P.seg2, P.tile2, P.ntile2, Y, P.status, s);
   timer.mark(2);
 }
