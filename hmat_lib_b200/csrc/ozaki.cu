@@ -308,27 +308,42 @@ __global__ void max_kernel(const MaxJob *__restrict__ jobs, int njobs, long long
   }
 }
 
-// Six slices of 16 consecutive K values of one line, scaled by 2^-ex, stored
-// as six aligned 16-byte words at `base` + p R 32.
+// Six slices of 16 consecutive K values of one line, stored as six aligned
+// 16-byte words at `base` + p R 32.  Each value is rounded once to the
+// integer N = x 2^(42 - ex) (|N| <= 127 2^35 because |x| 2^-ex <= 127/128)
+// and written in balanced base 128, N = sum_p d_p 128^(6-p): with
+// M = N + 2^42 + 64 (128^4 + ... + 1) >= 0, d_p = digit_p(M) - 64 for p > 1
+// (in [-64, 63]) and d_1 = (M >> 35) - 128 (in [-127, 127]).
 __device__ __forceinline__ void slice16(const double (&y0)[16], int ex, uint8_t *base, int R) {
-  int8_t out[kOzSlices][16];
+  constexpr long long kBias = (1LL << 42) + 64LL * ((1LL << 28) + (1LL << 21) + (1LL << 14) +
+                                                    (1LL << 7) + 1LL);
+  const int sh = 42 - ex;
+  const bool fast = sh >= -1022 && sh <= 1023;
+  const double scale = fast ? __longlong_as_double((long long)(sh + 1023) << 52) : 0.0;
+  uint32_t w[kOzSlices][4];
 #pragma unroll
-  for (int x = 0; x < 16; ++x) {
-    double y = ldexp(y0[x], -ex);
+  for (int q = 0; q < 4; ++q) {
+    uint32_t b[kOzSlices] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-    for (int p = 0; p < kOzSlices; ++p) {
-      y *= 128.0;
-      const double a = rint(y);
-      out[p][x] = (int8_t)a;
-      y -= a;
+    for (int x = 0; x < 4; ++x) {
+      const double v = y0[4 * q + x];
+      const long long N = __double2ll_rn(fast ? v * scale : ldexp(v, sh));
+      const unsigned long long M = (unsigned long long)(N + kBias);
+      const uint32_t lo = (uint32_t)M;                  // digits 4..6 (bits 0..20) and part of 3
+      const uint32_t hi = (uint32_t)(M >> 21);          // digits 1..3
+      const uint32_t d[kOzSlices] = {((hi >> 14) - 128u) & 0xFFu, (((hi >> 7) & 127u) - 64u) & 0xFFu,
+                                     ((hi & 127u) - 64u) & 0xFFu, (((lo >> 14) & 127u) - 64u) & 0xFFu,
+                                     (((lo >> 7) & 127u) - 64u) & 0xFFu, ((lo & 127u) - 64u) & 0xFFu};
+#pragma unroll
+      for (int p = 0; p < kOzSlices; ++p) b[p] |= d[p] << (8 * x);
     }
+#pragma unroll
+    for (int p = 0; p < kOzSlices; ++p) w[p][q] = b[p];
   }
 #pragma unroll
-  for (int p = 0; p < kOzSlices; ++p) {
-    int4 w;
-    memcpy(&w, out[p], 16);
-    *reinterpret_cast<int4 *>(base + (long long)p * R * kOzKBlock) = w;
-  }
+  for (int p = 0; p < kOzSlices; ++p)
+    *reinterpret_cast<uint4 *>(base + (long long)p * R * kOzKBlock) =
+        make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
 }
 
 // Line-contiguous sources: one item = 16 consecutive K positions of one
