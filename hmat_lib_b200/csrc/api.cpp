@@ -485,6 +485,60 @@ int hodlr_b200_check(hodlr_b200_tree t, void *stream) {
   }
 }
 
+int hodlr_b200_matmat_batched_dev(int count, const hodlr_b200_tree *trees, int op, int precision,
+                                  const double *const *d_x, const int *k, const int *ldx,
+                                  double *const *d_y, const int *ldy, void *stream) {
+  if (count < 0 || (count > 0 && (!trees || !d_x || !k || !ldx || !d_y || !ldy)) || op < 0 ||
+      op > 2)
+    return INPUT_ERROR;
+  try {
+    HB_REQUIRE(precision == HODLR_B200_FP64 || precision == HODLR_B200_MIXED, INPUT_ERROR,
+               "unknown precision mode");
+    std::vector<std::shared_ptr<DeviceTree>> ts;
+    std::vector<const double *> xs;
+    std::vector<double *> ys;
+    std::vector<int> ks;
+    std::vector<long long> lx, ly;
+    for (int i = 0; i < count; ++i) {
+      HB_REQUIRE(trees[i] != nullptr, INPUT_ERROR, "batched product: NULL tree");
+      ts.push_back(trees[i]->p);
+      xs.push_back(d_x[i]);
+      ys.push_back(d_y[i]);
+      ks.push_back(k[i]);
+      lx.push_back(ldx[i]);
+      ly.push_back(ldy[i]);
+    }
+    batched_product(ts, (ProdOp)op, (Precision)precision, xs, ks, lx, ys, ly, as_stream(stream));
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+int hodlr_b200_batched_tuning(char *buf, int capacity) {
+  const std::string t = batched_tuning();
+  if (buf && capacity > 0) {
+    const size_t n = std::min<size_t>(t.size(), (size_t)capacity - 1);
+    std::memcpy(buf, t.data(), n);
+    buf[n] = 0;
+  }
+  return (int)t.size();
+}
+
+int hodlr_b200_batched_check(void) {
+  try {
+    if (batched_status() != 0) {
+      set_last_error("a mixed-precision kernel gave up waiting on a barrier");
+      return SVD_FAILURE;
+    }
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+void hodlr_b200_batched_release(void) { batched_release(); }
+
 int hodlr_b200_build_stats(double *out, int capacity) {
   const BuildStats &st = last_build_stats();
   const double v[] = {(double)st.exact_blocks,     (double)st.sketched_blocks,

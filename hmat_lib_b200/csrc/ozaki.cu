@@ -411,6 +411,15 @@ __global__ void __launch_bounds__(256) slice_kcontig_kernel(const SliceJob *__re
   }
 }
 
+__global__ void ranges_kernel(const CopyRange *__restrict__ ranges) {
+  const CopyRange R = ranges[blockIdx.y];
+  auto *d = (unsigned long long *)R.dst;
+  auto *src = (const unsigned long long *)R.src;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < R.words;
+       i += (long long)gridDim.x * blockDim.x)
+    d[i] = src ? src[i] : 0ULL;
+}
+
 int grid_for(long long threads) {
   const long long cap = (long long)num_sms() * 8;
   return (int)std::max(1LL, std::min(cap, (threads + 255) / 256));
@@ -430,6 +439,13 @@ void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *
   const int grid = std::min(ntiles, num_sms());
   ozaki_gemm_kernel<<<grid, kThreads, kSmem, stream>>>(d_segs, d_tiles, ntiles, cbase, d_status);
   HB_LAUNCHED();
+}
+
+void ozaki_ranges(const CopyRange *d_ranges, int n, cudaStream_t stream) {
+  for (int off = 0; off < n; off += 65535) {
+    ranges_kernel<<<dim3(16, std::min(65535, n - off)), 256, 0, stream>>>(d_ranges + off);
+    HB_LAUNCHED();
+  }
 }
 
 MaxBatch ozaki_max_batch(std::vector<MaxJob> jobs, cudaStream_t stream) {

@@ -118,6 +118,15 @@ struct SliceBatch {
   long long items = 0;
   bool kcontig = false;
 };
+// Zero (src NULL) or copy `words` 8-byte words per range, all ranges in one
+// launch.
+struct CopyRange {
+  void *dst;
+  const void *src;
+  long long words;
+};
+void ozaki_ranges(const CopyRange *d_ranges, int n, cudaStream_t stream);
+
 MaxBatch ozaki_max_batch(std::vector<MaxJob> jobs, cudaStream_t stream);
 SliceBatch ozaki_slice_batch(std::vector<SliceJob> jobs, cudaStream_t stream);
 void ozaki_max(const MaxBatch &b, const double *xbase, cudaStream_t stream);

@@ -39,6 +39,72 @@ static int covering_block(int h, int i, int d, bool row_side) {
   return block_index(d, j, c);
 }
 
+void append_product(GemmBatch &p1, GemmBatch &p2, const DeviceTree &t, ProdOp op, int k,
+                    long long ldx, long long ldy, const ProductSlots &sl,
+                    const std::vector<long long> &w_off, int min_depth) {
+  const Geometry &g = t.g;
+  const int h = g.h;
+  const int A = sl.arena, X = sl.x, Y = sl.y, W = sl.w;
+  const long long ao = sl.arena_off, xo = sl.x_off, yo = sl.y_off, wo = sl.w_off;
+  // phase 1: projections
+  for (size_t bi = 0; bi < g.blocks.size(); ++bi) {
+    const BlockDesc &b = g.blocks[bi];
+    if (b.s == 0 || b.depth < min_depth) continue;
+    if (op == ProdOp::N) {          // W_b (s x k) = V_b^T X[c0 : c0 + n]
+      int p = p1.add(W, wo + w_off[bi], b.s, b.s, k);
+      p1.seg(p, A, ao + b.v_off, b.n, 1, X, xo + b.c0, ldx, 0, b.n);
+    } else if (op == ProdOp::T) {   // W_b (s x k) = U_b^T X[r0 : r0 + m]
+      int p = p1.add(W, wo + w_off[bi], b.s, b.s, k);
+      p1.seg(p, A, ao + b.u_off, b.m, 1, X, xo + b.r0, ldx, 0, b.m);
+    } else {                        // Z_b (k x s) = X[:, r0 : r0 + m] U_b
+      int p = p1.add(W, wo + w_off[bi], k, k, b.s);
+      p1.seg(p, X, xo + (long long)b.r0 * ldx, ldx, 0, A, ao + b.u_off, b.m, 0, b.m);
+    }
+  }
+  // phase 2: one problem per leaf row band (columns for op L)
+  for (int i = 0; i < g.nleaf(); ++i) {
+    const LeafDesc &L = t.leaves[i];
+    if (L.m == 0) continue;
+    if (op == ProdOp::N || op == ProdOp::T) {
+      int p = p2.add(Y, yo + L.r0, ldy, L.m, k);
+      p2.seg(p, A, ao + L.off, L.m, op == ProdOp::T ? 1 : 0, X, xo + L.r0, ldx, 0, L.m);
+      for (int d = h - 1; d >= min_depth; --d) {
+        const int bi = covering_block(h, i, d, op == ProdOp::N);
+        const BlockDesc &b = g.blocks[bi];
+        if (b.s == 0) continue;
+        if (op == ProdOp::N)
+          p2.seg(p, A, ao + b.u_off + (L.r0 - b.r0), b.m, 0, W, wo + w_off[bi], b.s, 0, b.s);
+        else
+          p2.seg(p, A, ao + b.v_off + (L.r0 - b.c0), b.n, 0, W, wo + w_off[bi], b.s, 0, b.s);
+      }
+    } else {
+      int p = p2.add(Y, yo + (long long)L.r0 * ldy, ldy, k, L.m);
+      p2.seg(p, X, xo + (long long)L.r0 * ldx, ldx, 0, A, ao + L.off, L.m, 0, L.m);
+      for (int d = h - 1; d >= min_depth; --d) {
+        const int bi = covering_block(h, i, d, false);
+        const BlockDesc &b = g.blocks[bi];
+        if (b.s == 0) continue;
+        p2.seg(p, W, wo + w_off[bi], k, 0, A, ao + b.v_off + (L.r0 - b.c0), b.n, 1, b.s);
+      }
+    }
+  }
+}
+
+long long product_w_layout(const DeviceTree &t, int k, std::vector<long long> &w_off) {
+  long long w_total = 0;
+  w_off.assign(t.g.blocks.size(), 0);
+  for (size_t b = 0; b < t.g.blocks.size(); ++b) {
+    w_off[b] = w_total;
+    w_total += align_up((long long)t.g.blocks[b].s * k);
+  }
+  return w_total;
+}
+
+TileShape default_shape(ProdOp op, int k, int phase) {
+  if (phase == 1) return (op == ProdOp::L) ? TileShape::M128N64 : TileShape::M64N128;
+  return (op == ProdOp::L && k <= 64) ? TileShape::M64N128 : TileShape::M128N64;
+}
+
 ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,
                           cudaStream_t stream, int min_depth) {
   std::lock_guard<std::mutex> lk(t.plan_mutex);
@@ -51,65 +117,15 @@ ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long l
   plan->k = k;
   plan->ldx = ldx;
   plan->ldy = ldy;
-  const Geometry &g = t.g;
-  const int h = g.h;
-  std::vector<long long> w_off(g.blocks.size(), 0);
-  long long w_total = 0;
-  for (size_t b = 0; b < g.blocks.size(); ++b) {
-    w_off[b] = w_total;
-    w_total += align_up((long long)g.blocks[b].s * k);
-  }
+  std::vector<long long> w_off;
+  const long long w_total = product_w_layout(t, k, w_off);
   plan->w_elems = w_total;
   HB_CUDA(cudaMalloc(&plan->w, std::max<long long>(w_total, 1) * sizeof(double)));
-
-  // phase 1: projections
-  GemmBatch p1;
-  for (size_t bi = 0; bi < g.blocks.size(); ++bi) {
-    const BlockDesc &b = g.blocks[bi];
-    if (b.s == 0 || b.depth < min_depth) continue;
-    if (op == ProdOp::N) {          // W_b (s x k) = V_b^T X[c0 : c0 + n]
-      int p = p1.add(kW, w_off[bi], b.s, b.s, k);
-      p1.seg(p, kArena, b.v_off, b.n, 1, kX, b.c0, ldx, 0, b.n);
-    } else if (op == ProdOp::T) {   // W_b (s x k) = U_b^T X[r0 : r0 + m]
-      int p = p1.add(kW, w_off[bi], b.s, b.s, k);
-      p1.seg(p, kArena, b.u_off, b.m, 1, kX, b.r0, ldx, 0, b.m);
-    } else {                        // Z_b (k x s) = X[:, r0 : r0 + m] U_b
-      int p = p1.add(kW, w_off[bi], k, k, b.s);
-      p1.seg(p, kX, (long long)b.r0 * ldx, ldx, 0, kArena, b.u_off, b.m, 0, b.m);
-    }
-  }
-  // phase 2: one problem per leaf row band (columns for op L)
-  GemmBatch p2;
-  for (int i = 0; i < g.nleaf(); ++i) {
-    const LeafDesc &L = t.leaves[i];
-    if (L.m == 0) continue;
-    if (op == ProdOp::N || op == ProdOp::T) {
-      int p = p2.add(kY, L.r0, ldy, L.m, k);
-      p2.seg(p, kArena, L.off, L.m, op == ProdOp::T ? 1 : 0, kX, L.r0, ldx, 0, L.m);
-      for (int d = h - 1; d >= min_depth; --d) {
-        const int bi = covering_block(h, i, d, op == ProdOp::N);
-        const BlockDesc &b = g.blocks[bi];
-        if (b.s == 0) continue;
-        if (op == ProdOp::N)
-          p2.seg(p, kArena, b.u_off + (L.r0 - b.r0), b.m, 0, kW, w_off[bi], b.s, 0, b.s);
-        else
-          p2.seg(p, kArena, b.v_off + (L.r0 - b.c0), b.n, 0, kW, w_off[bi], b.s, 0, b.s);
-      }
-    } else {
-      int p = p2.add(kY, (long long)L.r0 * ldy, ldy, k, L.m);
-      p2.seg(p, kX, (long long)L.r0 * ldx, ldx, 0, kArena, L.off, L.m, 0, L.m);
-      for (int d = h - 1; d >= min_depth; --d) {
-        const int bi = covering_block(h, i, d, false);
-        const BlockDesc &b = g.blocks[bi];
-        if (b.s == 0) continue;
-        p2.seg(p, kW, w_off[bi], k, 0, kArena, b.v_off + (L.r0 - b.c0), b.n, 1, b.s);
-      }
-    }
-  }
-  const TileShape s1 = (op == ProdOp::L) ? TileShape::M128N64 : TileShape::M64N128;
-  const TileShape s2 = (op == ProdOp::L && k <= 64) ? TileShape::M64N128 : TileShape::M128N64;
-  if (!p1.empty()) gemm_plan_build(plan->phase1, p1, s1, true, stream);
-  if (!p2.empty()) gemm_plan_build(plan->phase2, p2, s2, false, stream);
+  GemmBatch p1, p2;
+  append_product(p1, p2, t, op, k, ldx, ldy, ProductSlots{kArena, kX, kY, kW, 0, 0, 0, 0}, w_off,
+                 min_depth);
+  if (!p1.empty()) gemm_plan_build(plan->phase1, p1, default_shape(op, k, 1), true, stream);
+  if (!p2.empty()) gemm_plan_build(plan->phase2, p2, default_shape(op, k, 2), false, stream);
   auto &ref = *plan;
   t.plans[key] = std::move(plan);
   return ref;

@@ -1,6 +1,8 @@
 // HODLR x dense products on the device (FP64).
 #pragma once
 
+#include <string>
+
 #include "dtree.h"
 
 namespace hb {
@@ -54,6 +56,35 @@ void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double 
 // Error word of the tree's mixed-precision kernels (0: none), read and reset.
 int mixed_status(DeviceTree &t, cudaStream_t stream);
 
+// Mixed-precision products of many trees with one launch per step (each
+// tree at most once per batch: the tree's cached scratch is reused).
+struct MixedItem {
+  DeviceTree *t;
+  const double *X;
+  int k;
+  long long ldx;
+  double *Y;
+  long long ldy;
+};
+struct MixedBatch;
+struct MixedBatchDeleter {
+  void operator()(MixedBatch *b) const;
+};
+std::unique_ptr<MixedBatch, MixedBatchDeleter> mixed_batch_build(const std::vector<MixedItem> &items,
+                                                                 cudaStream_t stream);
+void mixed_batch_run(MixedBatch &b, cudaStream_t stream);
+int mixed_batch_status(MixedBatch &b, cudaStream_t stream);
+
+// Y_i = op(H_i) X_i for every i with one launch per phase (batched.cu).
+void batched_product(const std::vector<std::shared_ptr<DeviceTree>> &trees, ProdOp op,
+                     Precision prec, const std::vector<const double *> &X,
+                     const std::vector<int> &k, const std::vector<long long> &ldx,
+                     const std::vector<double *> &Y, const std::vector<long long> &ldy,
+                     cudaStream_t stream);
+int batched_status();            // worst error word of the cached mixed batches (read, reset)
+std::string batched_tuning();    // configuration the autotuner chose for the latest plan
+void batched_release();          // drops every cached batch plan
+
 // Events around the two phases of a product when option
 // "record_phase_times" is set (mark(1) after phase 1, mark(2) at the end).
 struct PhaseTimer {
@@ -68,6 +99,23 @@ struct PhaseTimer {
 // "record_phase_times" set: out[0] phase 1, out[1] phase 2, out[2] count.
 // Resets the accumulators.
 int phase_times(double *out, int cap);
+
+// Base slots and element offsets of one product's operands inside a GEMM
+// batch: a single tree uses its own slots with zero offsets; a batch of trees
+// addresses every operand from one common base.
+struct ProductSlots {
+  int arena, x, y, w;
+  long long arena_off, x_off, y_off, w_off;
+};
+
+// Appends one product's phase-1 and phase-2 problems (W laid out by w_off).
+void append_product(GemmBatch &p1, GemmBatch &p2, const DeviceTree &t, ProdOp op, int k,
+                    long long ldx, long long ldy, const ProductSlots &slots,
+                    const std::vector<long long> &w_off, int min_depth = 0);
+// Offsets of every block's W (s_b x k, or k x s_b for op L); returns the total.
+long long product_w_layout(const DeviceTree &t, int k, std::vector<long long> &w_off);
+// Tile shape used by the single-tree product for a phase (1 or 2).
+TileShape default_shape(ProdOp op, int k, int phase);
 
 // Builds (and caches on the tree) the plan for this shape without running it.
 ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,

@@ -109,6 +109,12 @@ struct MixedPlan {
   OzTile *tile1 = nullptr, *tile2 = nullptr;
   int ntile1 = 0, ntile2 = 0;
   int *status = nullptr;
+  // host copies for batches (X jobs with src NULL; phase-1 tiles relative to
+  // w, phase-2 tiles relative to Y)
+  std::vector<OzSeg> hs1, hs2;
+  std::vector<OzTile> ht1, ht2;
+  std::vector<MaxJob> hmx, hmw;
+  std::vector<SliceJob> hsx, hsxb, hsb;
   ~MixedPlan() {
     for (void *p : {(void *)xmax, (void *)fmax, (void *)xexp, (void *)fexp, (void *)xa, (void *)xb,
                     (void *)wb, (void *)w, (void *)max_x.d, (void *)max_wsplit.d, (void *)sl_xa.d,
@@ -390,6 +396,15 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   P.sl_xa = ozaki_slice_batch(sx, s);
   P.sl_xb = ozaki_slice_batch(sxb, s);
   P.sl_wb = ozaki_slice_batch(sb, s);
+  P.hs1 = s1;
+  P.hs2 = s2;
+  P.ht1 = t1s;
+  P.ht2 = t2;
+  P.hmx = mx;
+  P.hmw = mw;
+  P.hsx = sx;
+  P.hsxb = sxb;
+  P.hsb = sb;
   P.seg1 = upload(s1, s);
   P.tile1 = upload(t1s, s);
   P.ntile1 = (int)t1s.size();
@@ -428,6 +443,137 @@ void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double 
   ozaki_slice(P.sl_wb, X, s);
   ozaki_gemm(P.seg2, P.tile2, P.ntile2, Y, P.status, s);
   timer.mark(2);
+}
+
+// ---- many trees, one launch per step -------------------------------------------------
+
+struct MixedBatch {
+  double *base = nullptr;
+  CopyRange *pre = nullptr, *mid = nullptr;
+  int npre = 0, nmid = 0;
+  MaxBatch max_x, max_w;
+  SliceBatch sl_xa, sl_xb, sl_wb;
+  OzSeg *seg1 = nullptr, *seg2 = nullptr;
+  OzTile *tile1 = nullptr, *tile2 = nullptr;
+  int ntile1 = 0, ntile2 = 0;
+  int *status = nullptr;
+  ~MixedBatch() {
+    for (void *p : {(void *)pre, (void *)mid, (void *)max_x.d, (void *)max_w.d, (void *)sl_xa.d,
+                    (void *)sl_xb.d, (void *)sl_wb.d, (void *)seg1, (void *)seg2, (void *)tile1,
+                    (void *)tile2, (void *)status})
+      if (p) cudaFree(p);
+  }
+};
+
+void MixedBatchDeleter::operator()(MixedBatch *b) const { delete b; }
+
+std::unique_ptr<MixedBatch, MixedBatchDeleter> mixed_batch_build(const std::vector<MixedItem> &items,
+                                                                 cudaStream_t s) {
+  std::unique_ptr<MixedBatch, MixedBatchDeleter> B(new MixedBatch);
+  for (size_t i = 0; i < items.size(); ++i)
+    for (size_t j = 0; j < i; ++j)
+      HB_REQUIRE(items[i].t != items[j].t, INPUT_ERROR,
+                 "a mixed-precision batch takes each tree once");
+  std::vector<CopyRange> pre, mid;
+  std::vector<OzSeg> s1, s2;
+  std::vector<OzTile> t1, t2;
+  std::vector<long long> work1;
+  std::vector<MaxJob> mx, mw;
+  std::vector<SliceJob> sx, sxb, sb;
+  // outputs are addressed from the lowest output pointer
+  const double *base = nullptr;
+  std::vector<MixedPlan *> plans;
+  for (const MixedItem &it : items) {
+    DeviceTree &t = *it.t;
+    HB_REQUIRE(it.k > 0 && it.ldx >= t.g.n && it.ldy >= t.g.n, INPUT_ERROR,
+               "leading dimension below n");
+    std::lock_guard<std::mutex> lk(t.plan_mutex);
+    MixedState &st = mixed_state(t, s);
+    plans.push_back(&mixed_plan(t, st, it.k, it.ldx, it.ldy, s));
+    for (const double *p : {(const double *)plans.back()->w, (const double *)it.Y})
+      if (!base || p < base) base = p;
+  }
+  B->base = const_cast<double *>(base);
+  for (size_t i = 0; i < items.size(); ++i) {
+    const MixedItem &it = items[i];
+    MixedPlan &P = *plans[i];
+    pre.push_back(CopyRange{P.xmax, nullptr, it.k});
+    if (P.w_zero) pre.push_back(CopyRange{P.w, nullptr, P.w_zero});
+    mid.push_back(CopyRange{P.fmax, P.xmax, it.k});
+    const long long wrel = P.w - base, yrel = it.Y - base;
+    const int o1 = (int)s1.size(), o2 = (int)s2.size();
+    s1.insert(s1.end(), P.hs1.begin(), P.hs1.end());
+    s2.insert(s2.end(), P.hs2.begin(), P.hs2.end());
+    for (OzTile tl : P.ht1) {
+      work1.push_back((long long)P.hs1[tl.seg0].nkb * tl.nw);
+      tl.seg0 += o1;
+      tl.c_off += wrel;
+      t1.push_back(tl);
+    }
+    for (OzTile tl : P.ht2) {
+      tl.seg0 += o2;
+      tl.c_off += yrel;
+      t2.push_back(tl);
+    }
+    auto with_x = [&](std::vector<SliceJob> v, std::vector<SliceJob> &dst) {
+      for (SliceJob j : v) {
+        if (!j.src) j.src = it.X;
+        dst.push_back(j);
+      }
+    };
+    for (MaxJob j : P.hmx) {
+      if (!j.src) j.src = it.X;
+      mx.push_back(j);
+    }
+    mw.insert(mw.end(), P.hmw.begin(), P.hmw.end());
+    with_x(P.hsx, sx);
+    with_x(P.hsxb, sxb);
+    with_x(P.hsb, sb);
+  }
+  std::vector<int> order(t1.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work1[a] > work1[b]; });
+  std::vector<OzTile> t1s;
+  for (int i : order) t1s.push_back(t1[i]);
+  B->pre = upload(pre, s);
+  B->npre = (int)pre.size();
+  B->mid = upload(mid, s);
+  B->nmid = (int)mid.size();
+  B->max_x = ozaki_max_batch(mx, s);
+  B->max_w = ozaki_max_batch(mw, s);
+  B->sl_xa = ozaki_slice_batch(sx, s);
+  B->sl_xb = ozaki_slice_batch(sxb, s);
+  B->sl_wb = ozaki_slice_batch(sb, s);
+  B->seg1 = upload(s1, s);
+  B->seg2 = upload(s2, s);
+  B->tile1 = upload(t1s, s);
+  B->tile2 = upload(t2, s);
+  B->ntile1 = (int)t1s.size();
+  B->ntile2 = (int)t2.size();
+  B->status = dalloc<int>(1);
+  HB_CUDA(cudaMemsetAsync(B->status, 0, sizeof(int), s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  return B;
+}
+
+void mixed_batch_run(MixedBatch &B, cudaStream_t s) {
+  ozaki_ranges(B.pre, B.npre, s);
+  ozaki_max(B.max_x, nullptr, s);
+  ozaki_slice(B.sl_xa, nullptr, s);
+  ozaki_ranges(B.mid, B.nmid, s);
+  ozaki_gemm(B.seg1, B.tile1, B.ntile1, B.base, B.status, s);
+  ozaki_max(B.max_w, nullptr, s);
+  ozaki_slice(B.sl_xb, nullptr, s);
+  ozaki_slice(B.sl_wb, nullptr, s);
+  ozaki_gemm(B.seg2, B.tile2, B.ntile2, B.base, B.status, s);
+}
+
+int mixed_batch_status(MixedBatch &B, cudaStream_t s) {
+  int v = 0;
+  HB_CUDA(cudaMemcpyAsync(&v, B.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  HB_CUDA(cudaMemsetAsync(B.status, 0, sizeof(int), s));
+  return v;
 }
 
 int mixed_status(DeviceTree &t, cudaStream_t s) {

@@ -143,6 +143,26 @@ class Tree:
             pass
 
 
+def matmat_batched(trees, xs, ks, ldxs, ys, ldys, op: int = 0, precision: int = 0,
+                   stream: int = 0):
+    """hodlr_b200_matmat_batched_dev: Y_i = op(H_i) X_i for every tree, one
+    launch per phase.  xs / ys are device addresses (ints)."""
+    n = len(trees)
+    arr = lambda T, v: (T * max(n, 1))(*v)
+    r = lib().hodlr_b200_matmat_batched_dev(
+        n, arr(C.c_void_p, [t.h for t in trees]), op, precision, arr(C.c_void_p, xs),
+        arr(C.c_int, ks), arr(C.c_int, ldxs), arr(C.c_void_p, ys), arr(C.c_int, ldys),
+        C.c_void_p(stream))
+    if r != abi.SUCCESS:
+        raise HodlrError(r, "hodlr_b200_matmat_batched_dev", lib().hodlr_b200_last_error().decode())
+
+
+def batched_tuning() -> str:
+    buf = C.create_string_buffer(512)
+    lib().hodlr_b200_batched_tuning(buf, 512)
+    return buf.value.decode()
+
+
 class DeviceTree:
     """Handle of a device-resident tree (include/hmat_lib/hodlr_b200.h)."""
 

@@ -108,6 +108,31 @@ int hodlr_b200_matvec_noalloc_dev(hodlr_b200_tree t, const double *d_x, double *
 /* Re-upload a host tree whose factor values were edited in place. */
 int hodlr_b200_sync_tree(const struct TreeHODLR *hodlr);
 
+/* Y_i = op(H_i) X_i for i < count, every tree of the batch (any sizes, ranks
+ * and heights) in one launch per phase.  Device pointers, column-major;
+ * k[i] columns of X_i / Y_i (rows for op L), leading dimensions ldx[i],
+ * ldy[i].  precision HODLR_B200_MIXED needs op N, leaf sizes that are
+ * multiples of 32 and each tree at most once in the batch.  No counterpart in
+ * hmat_lib, which multiplies one tree at a time (multiply_hodlr_dense,
+ * src/dense_algebra.c:361).  The plan for a call signature (trees, pointers,
+ * sizes) is made on its first call: an autotuner times the candidate tile
+ * configurations on the real operands, and the chosen launches are captured
+ * into a CUDA graph that later calls with the same signature replay (option
+ * "autotune" = 0 keeps the default configuration, "use_graphs" = 0 launches
+ * directly).  Up to four plans are cached; a freed tree invalidates every plan
+ * that uses it.  Returns an ErrorCode. */
+int hodlr_b200_matmat_batched_dev(int count, const hodlr_b200_tree *trees, int op, int precision,
+                                  const double *const *d_x, const int *k, const int *ldx,
+                                  double *const *d_y, const int *ldy, void *stream);
+/* Configuration the autotuner chose for the latest batched plan, written to
+ * buf (NUL-terminated, at most capacity bytes); returns its full length. */
+int hodlr_b200_batched_tuning(char *buf, int capacity);
+/* SUCCESS, or SVD_FAILURE if a cached mixed-precision batch hit a barrier
+ * timeout (read and reset). */
+int hodlr_b200_batched_check(void);
+/* Drops every cached batched plan (their graphs and scratch). */
+void hodlr_b200_batched_release(void);
+
 #ifdef __cplusplus
 }
 #endif
