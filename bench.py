@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--n", type=int, default=None, help="override n (testing only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=4096)
+    ap.add_argument("--batch", type=int, default=512,
+                    help="instances of the uneven-batch measurement (0: skip)")
     return ap.parse_args()
 
 
@@ -165,6 +167,93 @@ def run_cpu_baseline(n: int, k: int):
         return json.loads(line)
     except Exception as e:  # the baseline is reported, never required
         return {"error": str(e)[:200]}
+
+
+def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream):
+    """The uneven batch: `count` HODLRs (n in {1024, 2048, 4096, 8192},
+    exponential kernel on sorted 1D points, leaf 128, tol 1e-8), each times a
+    dense block of 16-128 columns.  Times one step (all instances) three ways:
+    one FP64 product call per tree, the batched FP64 call and the batched
+    mixed-precision call (one launch per phase, graph replay)."""
+    import numpy as np
+
+    from hmat_lib_b200 import workloads as W
+    from hmat_lib_b200.hodlr import DeviceTree, batched_tuning, matmat_batched
+    sh = stream.cuda_stream
+    inst = W.uneven_batch(count, seed=2)
+    nmax = max(it["n"] for it in inst)
+    trees, xs, ys, ks, ns = [], [], [], [], []
+    build_s = 0.0
+    with torch.cuda.stream(stream):
+        a = torch.empty(nmax * nmax, dtype=torch.float64, device=dev)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(2)
+        for it in inst:
+            n, k = it["n"], it["k"]
+            d_pts = torch.from_numpy(np.ascontiguousarray(it["points"][:, 0])).to(dev)
+            r = lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, 1, 2,
+                                                 it["length"], 0.0, C.c_void_p(a.data_ptr()), n,
+                                                 C.c_void_p(sh))
+            assert r == 0
+            stream.synchronize()
+            t0 = time.perf_counter()
+            trees.append(DeviceTree.build(a.data_ptr(), n, n, it["height"], it["tol"], stream=sh))
+            build_s += time.perf_counter() - t0
+            xs.append(torch.randn(k, n, dtype=torch.float64, device=dev, generator=gen))
+            ys.append(torch.zeros(k, n, dtype=torch.float64, device=dev))
+            ks.append(k)
+            ns.append(n)
+        del a
+    torch.cuda.empty_cache()
+    storage = sum(t.info()["storage"] for t in trees)
+    bytes_step = 8.0 * storage + sum(16.0 * n * k for n, k in zip(ns, ks))
+    xp, yp = [x.data_ptr() for x in xs], [y.data_ptr() for y in ys]
+
+    def loop_step():
+        for t, x, y, n, k in zip(trees, xs, ys, ns, ks):
+            t.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
+
+    def batched_step(precision, out):
+        matmat_batched(trees, xp, ks, ns, out, ns, precision=precision, stream=sh)
+
+    def timed(fn, nsteps):
+        for _ in range(warmup):
+            fn()
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = lib.hodlr_b200_kernel_launches()
+        e0.record(stream)
+        for _ in range(nsteps):
+            fn()
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / nsteps
+        return {"ms_per_step": ms, "GB/s": bytes_step / (ms * 1e-3) / 1e9,
+                "gpu_launches_per_step": (lib.hodlr_b200_kernel_launches() - l0) / nsteps}
+
+    nsteps = max(5, steps // 8)
+    loop = timed(loop_step, max(3, nsteps // 4))
+    y64 = [y.clone() for y in ys]
+    b64 = timed(lambda: batched_step(0, yp), nsteps)
+    tuning = batched_tuning()
+    y64b = [y.clone() for y in ys]
+    ymx = [torch.zeros_like(y) for y in ys]
+    bmx = timed(lambda: batched_step(1, [y.data_ptr() for y in ymx]), nsteps)
+    assert lib.hodlr_b200_batched_check() == 0, lib.hodlr_b200_last_error()
+    num = sum(float(torch.linalg.norm(m - f) ** 2) for m, f in zip(ymx, y64b))
+    den = sum(float(torch.linalg.norm(f) ** 2) for f in y64b)
+    numb = sum(float(torch.linalg.norm(b - f) ** 2) for b, f in zip(y64b, y64))
+    out = {"instances": count, "sizes": sorted(set(ns)), "k_range": [min(ks), max(ks)],
+           "kernel": "exp(-|x-y|/l), l ~ U[0.05,0.5], sorted 1D points, seed 2",
+           "build_s_total": build_s, "storage_doubles": storage, "bytes_per_step": bytes_step,
+           "loop_fp64": loop, "batched_fp64": b64, "batched_mixed": bmx,
+           "speedup_batched_mixed_vs_loop_fp64": loop["ms_per_step"] / bmx["ms_per_step"],
+           "rel_err_batched_fp64_vs_loop": (numb / den) ** 0.5,
+           "rel_err_mixed_vs_fp64": (num / den) ** 0.5, "tuning": tuning}
+    lib.hodlr_b200_batched_release()
+    for t in trees:
+        t.free()
+    return out
 
 
 def reference_arm(args, rank):
@@ -349,6 +438,10 @@ def main():
     e2e_s = e2e_time(1)
     e2e = bytes_step * world / e2e_s / 1e9
 
+    batch = None
+    if args.batch > 0:
+        batch = uneven_batch_bench(args.batch, args.steps, args.warmup, lib, torch, dev, stream)
+
     if rank != 0:
         if pg:
             pg.destroy_process_group()
@@ -429,6 +522,7 @@ def main():
                 "path": "multiply_hodlr_dense, option matmat_precision=1"},
         "gpu_launches": rmx["launches"],
         "cpu_baseline": cpu,
+        "batch": batch,
     }
     print(json.dumps(line))
     host_tree.free()

@@ -111,7 +111,9 @@ float time_best(F fn, cudaStream_t s, int reps = 3) {
   return best;
 }
 
-const char *shape_name(TileShape t) { return t == TileShape::M128N64 ? "128x64" : "64x128"; }
+std::string shape_name(TileShape t) {
+  return std::to_string(tile_rows(t)) + "x" + std::to_string(tile_cols(t));
+}
 
 // Plans phase `phase` of the FP64 batch for every candidate configuration,
 // times them on the real operands, keeps the fastest.
@@ -123,8 +125,12 @@ std::unique_ptr<GemmPlan> tune_phase(const GemmBatch &batch, int phase, ProdOp o
     bool split;
   };
   std::vector<Cand> cands;
-  if (autotune) {
-    for (TileShape sh : {TileShape::M128N64, TileShape::M64N128})
+  const int forced = (int)option("batch_shape", -1.0);   // 0..3: one shape, no timing
+  if (forced >= 0 && forced <= 3) {
+    cands.push_back(Cand{(TileShape)forced, phase == 1});
+  } else if (autotune) {
+    for (TileShape sh : {TileShape::M128N64, TileShape::M64N128, TileShape::M32N128,
+                         TileShape::M32N256})
       for (bool sp : {false, true}) cands.push_back(Cand{sh, sp});
   } else {
     cands.push_back(Cand{default_shape(op, kmax, phase), phase == 1});

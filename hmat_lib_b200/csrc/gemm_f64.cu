@@ -1,7 +1,7 @@
 // FP64 variable-batched segmented GEMM for sm_100a.
 //
 // CUDA-core DFMA kernel: 256 threads, a BM x BN output tile per CTA
-// (128 x 64 or 64 x 128), K advanced 16 at a time through a two-stage
+// (128 x 64, 64 x 128, 32 x 128 or 32 x 256), K advanced 16 at a time through a two-stage
 // cp.async pipeline (8-byte copies with zero fill, so any leading dimension
 // and any offset work), 32 accumulators per thread, operands read from shared
 // memory as double2.  FP64 has no tcgen05 path; this is the FP64 roofline
@@ -237,8 +237,8 @@ GemmPlan::~GemmPlan() {
 
 void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool allow_split,
                      cudaStream_t stream) {
-  const int BM = shape == TileShape::M128N64 ? 128 : 64;
-  const int BN = shape == TileShape::M128N64 ? 64 : 128;
+  const int BM = tile_rows(shape);
+  const int BN = tile_cols(shape);
   plan.shape = shape;
   auto &probs = batch.probs;
   std::vector<long long> ktot(probs.size(), 0);
@@ -322,10 +322,12 @@ void gemm_plan_run(const GemmPlan &plan, const GemmBases &bases, cudaStream_t st
     gemm_scale_c_kernel<<<grid, 256, 0, stream>>>(plan.probs, plan.nprobs, bases);
     HB_LAUNCHED();
   }
-  if (plan.shape == TileShape::M128N64)
-    launch_gemm<128, 64>(plan, bases, stream);
-  else
-    launch_gemm<64, 128>(plan, bases, stream);
+  switch (plan.shape) {
+    case TileShape::M128N64: launch_gemm<128, 64>(plan, bases, stream); break;
+    case TileShape::M64N128: launch_gemm<64, 128>(plan, bases, stream); break;
+    case TileShape::M32N128: launch_gemm<32, 128>(plan, bases, stream); break;
+    case TileShape::M32N256: launch_gemm<32, 256>(plan, bases, stream); break;
+  }
 }
 
 void gemm_f64_run(GemmBatch &batch, const GemmBases &bases, TileShape shape, cudaStream_t stream,

@@ -50,7 +50,15 @@ struct GemmTile {
   int k0, k1;           // range in the problem's concatenated K index
 };
 
-enum class TileShape { M128N64 = 0, M64N128 = 1 };
+// Output tile per CTA.  The 32-row shapes serve skinny problems (a few rows:
+// the projections V^T X of low-rank blocks).
+enum class TileShape { M128N64 = 0, M64N128 = 1, M32N128 = 2, M32N256 = 3 };
+inline int tile_rows(TileShape t) {
+  return t == TileShape::M128N64 ? 128 : t == TileShape::M64N128 ? 64 : 32;
+}
+inline int tile_cols(TileShape t) {
+  return t == TileShape::M128N64 ? 64 : t == TileShape::M32N256 ? 256 : 128;
+}
 
 struct GemmBatch {
   std::vector<GemmSeg> segs;

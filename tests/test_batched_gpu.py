@@ -146,6 +146,28 @@ def test_without_autotune_or_graphs(batch):
         lib.hodlr_b200_set_option(b"use_graphs", 1.0)
 
 
+@pytest.mark.parametrize("shape", [0, 1, 2, 3], ids=["128x64", "64x128", "32x128", "32x256"])
+def test_every_tile_shape(batch, shape):
+    """Each tile shape the autotuner may pick gives the same products."""
+    import torch
+    lib = abi.load()
+    trees, meta = batch
+    lib.hodlr_b200_set_option(b"batch_shape", float(shape))
+    try:
+        for op in (0, 2):
+            xs, ys = _buffers(meta[:6], op, seed=70 + shape)
+            ks = [x.shape[0] if op == 2 else x.shape[1] for x in xs]
+            matmat_batched(trees[:6], [x.data_ptr() for x in xs], ks, [_ld(x) for x in xs],
+                           [y.data_ptr() for y in ys], [_ld(y) for y in ys], op=op)
+            torch.cuda.synchronize()
+            for dt, x, y in zip(trees[:6], xs, ys):
+                want = _single(dt, x, op)
+                torch.cuda.synchronize()
+                assert O.rel_fro(y.cpu().numpy(), want.cpu().numpy()) < 1e-13
+    finally:
+        lib.hodlr_b200_set_option(b"batch_shape", -1.0)
+
+
 def test_batched_mixed(batch):
     """Mixed precision: every tree once, results within the slicing error of
     each tree's FP64 product."""
