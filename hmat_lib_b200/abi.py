@@ -31,6 +31,7 @@ ERROR_NAMES = {
 }
 
 DP = C.POINTER(C.c_double)
+FP = C.POINTER(C.c_float)
 
 
 class NodeDiagonal(C.Structure):
@@ -142,6 +143,15 @@ B200_API = {
     "hodlr_b200_batched_tuning": (C.c_int, [C.c_char_p, C.c_int]),
     "hodlr_b200_batched_check": (C.c_int, []),
     "hodlr_b200_batched_release": (None, []),
+    "hodlr_b200_rank_model_size": (C.c_int, []),
+    "hodlr_b200_rank_model_set": (C.c_int, [FP, C.c_int]),
+    "hodlr_b200_rank_model_get": (C.c_int, [FP, C.c_int]),
+    "hodlr_b200_rank_model_train": (
+        C.c_int, [FP, FP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, FP, FP, C.c_int]),
+    "hodlr_b200_rank_model_predict": (C.c_int, [FP, FP, C.c_int, FP]),
+    "hodlr_b200_rank_model_gradient": (C.c_int, [FP, FP, FP, C.c_int, FP, FP]),
+    "hodlr_b200_rank_model_adam": (C.c_int, [FP, FP, FP, FP, C.c_int, C.c_double]),
+    "hodlr_b200_build_features": (C.c_int, [FP, C.c_int]),
 }
 
 

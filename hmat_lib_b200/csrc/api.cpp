@@ -16,6 +16,7 @@
 #include "build.h"
 #include "hxh.h"
 #include "products.h"
+#include "rank_mlp.h"
 
 using namespace hb;
 
@@ -539,13 +540,140 @@ int hodlr_b200_batched_check(void) {
 
 void hodlr_b200_batched_release(void) { batched_release(); }
 
+// ---------------------------------------------------------------- rank model
+
+namespace {
+struct DevFloats {
+  float *p = nullptr;
+  cudaStream_t s;
+  DevFloats(const float *host, size_t n, cudaStream_t st) : s(st) {
+    HB_CUDA(cudaMallocAsync((void **)&p, sizeof(float) * std::max<size_t>(n, 1), s));
+    if (host && n)
+      HB_CUDA(cudaMemcpyAsync(p, host, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+  }
+  void to_host(float *host, size_t n) {
+    if (host && n) HB_CUDA(cudaMemcpyAsync(host, p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+  }
+  ~DevFloats() { cudaFreeAsync(p, s); }
+};
+}  // namespace
+
+int hodlr_b200_rank_model_size(void) { return kRankParams; }
+
+int hodlr_b200_rank_model_set(const float *params, int count) {
+  if (count == 0) {
+    set_rank_model({});
+    return SUCCESS;
+  }
+  if (!params || count != kRankParams) {
+    set_last_error("rank model: wrong parameter count");
+    return INPUT_ERROR;
+  }
+  set_rank_model(std::vector<float>(params, params + count));
+  return SUCCESS;
+}
+
+int hodlr_b200_rank_model_get(float *params, int capacity) {
+  std::vector<float> m;
+  if (!rank_model(m)) return 0;
+  if (params) std::copy(m.begin(), m.begin() + std::min<int>(capacity, (int)m.size()), params);
+  return (int)m.size();
+}
+
+int hodlr_b200_rank_model_train(const float *features, const float *targets, int n, int steps,
+                                int batch, double lr, unsigned long long seed, float *params_out,
+                                float *loss_log, int log_capacity) {
+  if (!features || !targets || !params_out || n <= 0 || steps <= 0 || batch <= 0)
+    return INPUT_ERROR;
+  try {
+    RankTrainConfig cfg;
+    cfg.steps = steps;
+    cfg.batch = batch;
+    cfg.lr = (float)lr;
+    cfg.seed = seed;
+    std::vector<float> loss;
+    std::vector<float> P = rank_mlp_train(std::vector<float>(features, features + (size_t)n * kRankIn),
+                                          std::vector<float>(targets, targets + n), cfg, &loss,
+                                          lib_stream());
+    std::copy(P.begin(), P.end(), params_out);
+    for (int i = 0; loss_log && i < log_capacity && i < (int)loss.size(); ++i) loss_log[i] = loss[i];
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+int hodlr_b200_rank_model_predict(const float *params, const float *features, int n, float *out) {
+  if (!params || !features || !out || n < 0) return INPUT_ERROR;
+  try {
+    cudaStream_t s = lib_stream();
+    DevFloats dp(params, kRankParams, s), dx(features, (size_t)n * kRankIn, s), dy(nullptr, n, s);
+    rank_mlp_predict(dp.p, dx.p, n, dy.p, s);
+    dy.to_host(out, n);
+    HB_CUDA(cudaStreamSynchronize(s));
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+int hodlr_b200_rank_model_gradient(const float *params, const float *features,
+                                   const float *targets, int n, float *grad_out,
+                                   float *loss_out) {
+  if (!params || !features || !targets || !grad_out || n <= 0) return INPUT_ERROR;
+  try {
+    cudaStream_t s = lib_stream();
+    DevFloats dp(params, kRankParams, s), dx(features, (size_t)n * kRankIn, s),
+        dt(targets, n, s), dg(nullptr, kRankParams, s), dl(nullptr, 1, s);
+    rank_mlp_gradient(dp.p, dx.p, dt.p, n, dg.p, dl.p, s);
+    dg.to_host(grad_out, kRankParams);
+    dl.to_host(loss_out, loss_out ? 1 : 0);
+    HB_CUDA(cudaStreamSynchronize(s));
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+int hodlr_b200_rank_model_adam(float *params, const float *grad, float *m, float *v, int step,
+                               double lr) {
+  if (!params || !grad || !m || !v || step < 1) return INPUT_ERROR;
+  try {
+    cudaStream_t s = lib_stream();
+    DevFloats dp(params, kRankParams, s), dg(grad, kRankParams, s), dm(m, kRankParams, s),
+        dv(v, kRankParams, s);
+    RankTrainConfig cfg;
+    cfg.lr = (float)lr;
+    rank_mlp_adam(dp.p, dg.p, dm.p, dv.p, step, cfg, s);
+    dp.to_host(params, kRankParams);
+    dm.to_host(m, kRankParams);
+    dv.to_host(v, kRankParams);
+    HB_CUDA(cudaStreamSynchronize(s));
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+int hodlr_b200_build_features(float *out, int capacity_rows) {
+  const std::vector<float> &f = last_build_features();
+  const int rows = (int)(f.size() / kFeatureRow);
+  if (out)
+    std::copy(f.begin(), f.begin() + (size_t)std::min(rows, std::max(capacity_rows, 0)) * kFeatureRow,
+              out);
+  return rows;
+}
+
 int hodlr_b200_build_stats(double *out, int capacity) {
   const BuildStats &st = last_build_stats();
   const double v[] = {(double)st.exact_blocks,     (double)st.sketched_blocks,
                       (double)st.sketch_rounds,    st.seconds,
                       (double)st.cap_hit,          (double)st.max_sweeps_exact,
                       (double)st.max_sweeps_sketch, (double)st.failed_exact,
-                      (double)st.failed_sketch,    (double)st.max_sketch};
+                      (double)st.failed_sketch,    (double)st.max_sketch,
+                      st.ms_exact,                 st.ms_rounds,
+                      st.ms_core_svd,              st.ms_finish,
+                      (double)st.learned_fallbacks};
   const int n = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < n && i < capacity && out; ++i) out[i] = v[i];
   return n;

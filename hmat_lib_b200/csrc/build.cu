@@ -24,6 +24,7 @@
 
 #include "build.h"
 #include "jacobi.h"
+#include "rank_mlp.h"
 #include "tsqr.h"
 
 namespace hb {
@@ -50,13 +51,114 @@ struct SketchBlock {
   bool done = false;
   double sig_lb = 0.0;   // lower bound of sigma_0: largest row norm of B
   int last_pw = 0;
+  int first_w = 0;       // width of the first round (predicted, or sketch_first)
+  int pred = -1;         // predicted rank (-1: none)
+  bool one_shot = false; // first round sized by the predictor, judged at tol
+  bool fell_back = false;
 };
 
 thread_local BuildStats g_last_stats;
+thread_local std::vector<float> g_last_features;
+
+constexpr int kFeatCols = 16;   // width of the feature sketch
+
+// Rank-model features of every sketched block (rank_mlp.h): a 16-column
+// Gaussian sketch Y = A_b Omega, its singular values by the batched Jacobi
+// SVD, then log block size, depth, ln(kernel length) and five log ratios of
+// the sketch's singular values.
+std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlock> &sk,
+                                  const double *d_A, long long lda, unsigned long long seed,
+                                  cudaStream_t stream) {
+  const int nsk = (int)sk.size();
+  std::vector<float> f((size_t)nsk * kRankIn, 0.f);
+  if (nsk == 0) return f;
+  long long total = 0;
+  std::vector<long long> om(nsk), y(nsk), ws(nsk), u(nsk), v(nsk), sg(nsk);
+  for (int i = 0; i < nsk; ++i) {
+    const SketchBlock &S = sk[i];
+    auto take = [&](long long e) {
+      const long long o = total;
+      total += align_up(std::max<long long>(e, 1));
+      return o;
+    };
+    om[i] = take((long long)S.n * kFeatCols);
+    y[i] = take((long long)S.m * kFeatCols);
+    ws[i] = take(jacobi_workspace(S.m, kFeatCols));
+    u[i] = take((long long)S.m * kFeatCols);
+    v[i] = take(kFeatCols * kFeatCols);
+    sg[i] = take(kFeatCols);
+  }
+  double *w = dev_alloc(total, stream);
+  int *d_rank = nullptr;
+  HB_CUDA(cudaMallocAsync((void **)&d_rank, sizeof(int) * (nsk + 1), stream));
+  HB_CUDA(cudaMemsetAsync(d_rank, 0, sizeof(int) * (nsk + 1), stream));
+  std::vector<RandDesc> rd;
+  for (int i = 0; i < nsk; ++i)
+    rd.push_back(RandDesc{w + om[i], sk[i].n, sk[i].n, kFeatCols,
+                          (1ULL << 60) + ((unsigned long long)sk[i].b << 8)});
+  gaussian_fill(rd, seed, stream);
+  GemmBases bases{};
+  bases.p[0] = const_cast<double *>(d_A);
+  for (int i = 1; i < kGemmBases; ++i) bases.p[i] = w;
+  GemmBatch gb;
+  for (int i = 0; i < nsk; ++i) {
+    const SketchBlock &S = sk[i];
+    int pr = gb.add(1, y[i], S.m, S.m, kFeatCols);
+    gb.seg(pr, 0, S.a_off, lda, 0, 1, om[i], S.n, 0, S.n);
+  }
+  gemm_f64_run(gb, bases, TileShape::M128N64, stream);
+  std::vector<JacobiProb> jp;
+  for (int i = 0; i < nsk; ++i) {
+    const SketchBlock &S = sk[i];
+    JacobiProb q{};
+    q.A = w + y[i];
+    q.lda = S.m;
+    q.m = S.m;
+    q.n = kFeatCols;
+    q.G = w + ws[i];
+    q.W = q.G + align_up((long long)S.m * kFeatCols);
+    q.U = w + u[i];
+    q.ldu = S.m;
+    q.V = w + v[i];
+    q.ldv = kFeatCols;
+    q.sigma = w + sg[i];
+    q.rank = d_rank + i;
+    jp.push_back(q);
+  }
+  JacobiParams prm;
+  prm.trunc = Truncation::None;
+  prm.max_sweeps = 30;
+  JacobiProb *d_jp = upload_vec(jp, stream);
+  jacobi_svd_batched(d_jp, nsk, prm, d_rank + nsk, kFeatCols, stream);
+  std::vector<double> sig((size_t)nsk * kFeatCols);
+  for (int i = 0; i < nsk; ++i)
+    HB_CUDA(cudaMemcpyAsync(&sig[(size_t)i * kFeatCols], w + sg[i], sizeof(double) * kFeatCols,
+                            cudaMemcpyDeviceToHost, stream));
+  HB_CUDA(cudaStreamSynchronize(stream));
+  cudaFreeAsync(d_jp, stream);
+  cudaFreeAsync(d_rank, stream);
+  dev_free(w, stream);
+  const double length = option("kernel_length", 0.0);
+  for (int i = 0; i < nsk; ++i) {
+    const SketchBlock &S = sk[i];
+    float *row = &f[(size_t)i * kRankIn];
+    row[0] = (float)std::log2((double)std::min(S.m, S.n));
+    row[1] = (float)g.blocks[S.b].depth;
+    row[2] = length > 0.0 ? (float)std::log(length) : 0.f;
+    const double *sv = &sig[(size_t)i * kFeatCols];
+    const int idx[5] = {1, 3, 7, 11, 15};   // s_2, s_4, s_8, s_12, s_16
+    for (int q = 0; q < 5; ++q) {
+      const double r = sv[0] > 0.0 ? sv[idx[q]] / sv[0] : 0.0;
+      row[3 + q] = (float)std::max(-20.0, r > 0.0 ? std::log10(r) : -20.0);
+    }
+  }
+  return f;
+}
 
 }  // namespace
 
 const BuildStats &last_build_stats() { return g_last_stats; }
+const std::vector<float> &last_build_features() { return g_last_features; }
 
 std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double *d_A,
                                              long long lda, double tol, cudaStream_t stream,
@@ -103,7 +205,6 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     max_c = std::max(max_c, C);
   }
   std::vector<SketchBlock> sk;
-  const int w_max = std::max(w_first, w_next);
   for (int b : sketched) {
     const BlockDesc &B = g.blocks[b];
     SketchBlock S;
@@ -112,16 +213,63 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     S.n = B.n;
     S.cap = std::min(std::min(B.m, B.n), std::max(cap_max, kPanel));
     S.a_off = B.r0 + (long long)B.c0 * lda;
-    S.q = take((long long)B.m * S.cap);
-    S.bt = take((long long)B.n * S.cap);
-    S.p = take((long long)B.n * S.cap);
-    S.rb = take((long long)S.cap * S.cap);
-    S.om = take((long long)B.n * w_max);
-    S.t = take((long long)S.cap * w_max);
-    S.c = take((long long)S.cap * kPanel);
-    S.rn = take((long long)kPanel * kPanel + kPanel + w_max);
     sk.push_back(S);
   }
+  // ---- learned sizing of the first sketch ---------------------------------------------
+  const bool learned = option("learned_ranks", 0.0) != 0.0;
+  const bool record = learned || option("record_features", 0.0) != 0.0;
+  std::vector<float> feats;
+  std::vector<float> model;
+  const bool have_model = learned && rank_model(model);
+  for (SketchBlock &S : sk) S.first_w = std::min(w_first, S.cap);
+  if (record && !sk.empty()) {
+    feats = block_features(g, sk, d_A, lda, seed, stream);
+    if (have_model) {
+      const int nsk = (int)sk.size();
+      float *dbuf = nullptr;
+      HB_CUDA(cudaMallocAsync((void **)&dbuf, sizeof(float) * (kRankParams + nsk * (kRankIn + 1)),
+                              stream));
+      HB_CUDA(cudaMemcpyAsync(dbuf, model.data(), sizeof(float) * kRankParams,
+                              cudaMemcpyHostToDevice, stream));
+      HB_CUDA(cudaMemcpyAsync(dbuf + kRankParams, feats.data(), sizeof(float) * nsk * kRankIn,
+                              cudaMemcpyHostToDevice, stream));
+      float *dout = dbuf + kRankParams + nsk * kRankIn;
+      rank_mlp_predict(dbuf, dbuf + kRankParams, nsk, dout, stream);
+      std::vector<float> pred(nsk);
+      HB_CUDA(cudaMemcpyAsync(pred.data(), dout, sizeof(float) * nsk, cudaMemcpyDeviceToHost,
+                              stream));
+      HB_CUDA(cudaStreamSynchronize(stream));
+      cudaFreeAsync(dbuf, stream);
+      // one-shot width: the predicted rank plus a margin, whole panels
+      const double rel = option("learned_margin", 0.1);
+      const int add = (int)option("learned_extra", 40);
+      for (int i = 0; i < nsk; ++i) {
+        SketchBlock &S = sk[i];
+        const double r = std::max(1.0, std::exp2((double)std::min(pred[i], 20.f)) - 1.0);
+        S.pred = (int)std::lround(r);
+        const int w = (int)std::ceil(r * (1.0 + rel)) + add;
+        S.first_w = std::min(S.cap, std::max(kPanel, (w + kPanel - 1) / kPanel * kPanel));
+        S.one_shot = true;
+      }
+    }
+  }
+  // scratch of the sketched blocks: test matrices and products as wide as a
+  // block's widest round
+  int w_max = std::max(w_first, w_next);
+  for (SketchBlock &S : sk) {
+    const int wb = std::max(S.first_w, w_next);
+    w_max = std::max(w_max, wb);
+    S.q = take((long long)S.m * S.cap);
+    S.bt = take((long long)S.n * S.cap);
+    S.p = take((long long)S.n * S.cap);
+    S.rb = take((long long)S.cap * S.cap);
+    S.om = take((long long)S.n * wb);
+    S.t = take((long long)S.cap * wb);
+    S.c = take((long long)S.cap * kPanel);
+    S.rn = take((long long)kPanel * kPanel + kPanel + wb);
+  }
+  const double eta_learned = option("learned_eta", 1.0);
+
   double *work = dev_alloc(scratch, stream);
   GemmBases bases{};
   bases.p[kA] = const_cast<double *>(d_A);
@@ -142,6 +290,11 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   prm.trunc = Truncation::Relative;
   prm.scale_u = 1;
   prm.max_sweeps = (int)option("jacobi_max_sweeps", 60);
+
+  // stage events: start, exact done, rounds done, core SVDs done, end
+  cudaEvent_t ev[5];
+  for (auto &e : ev) HB_CUDA(cudaEventCreate(&e));
+  HB_CUDA(cudaEventRecord(ev[0], stream));
 
   // ---- exact path ----------------------------------------------------------------
   std::vector<JacobiProb> eprobs;
@@ -171,6 +324,8 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     jacobi_svd_batched(d_eprobs, (int)eprobs.size(), prm, d_status, max_c, stream);
   }
 
+  HB_CUDA(cudaEventRecord(ev[1], stream));
+
   // ---- sketched path ---------------------------------------------------------------
   int rounds = 0;
   bool cap_hit = false;
@@ -180,9 +335,9 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     for (size_t i = 0; i < sk.size(); ++i)
       if (!sk[i].done) act.push_back((int)i);
     if (act.empty()) break;
-    const int wr = rounds == 0 ? w_first : w_next;
     std::vector<int> wb(sk.size(), 0);
     for (int i : act) {
+      const int wr = rounds == 0 ? sk[i].first_w : w_next;
       wb[i] = std::min(wr, sk[i].cap - sk[i].ell);
       if (wb[i] <= 0) {
         sk[i].done = true;
@@ -366,13 +521,21 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
       for (int c = 0; c < wb[act[a]]; ++c) S.sig_lb = std::max(S.sig_lb, std::sqrt(bn[a * w_max + c]));
       S.ell += wb[act[a]];
       const double res = std::sqrt(f2 / std::max(S.last_pw, 1));
-      // stop at the tolerance, or at the FP64 noise floor of the estimate
-      const double floor_rel = std::max(eta * tol, 1e-14);
+      // stop at the tolerance, or at the FP64 noise floor of the estimate; a
+      // one-shot sketch sized by the predictor is accepted when the estimate
+      // is within the tolerance itself, otherwise the block continues with
+      // the plain adaptive rule
+      const bool first_shot = S.one_shot && rounds == 0;
+      const double floor_rel = std::max((first_shot ? eta_learned : eta) * tol, 1e-14);
       if (S.ell >= std::min(S.m, S.n) || S.sig_lb == 0.0 || res <= floor_rel * S.sig_lb)
         S.done = true;
+      else if (first_shot)
+        S.fell_back = true;
     }
     ++rounds;
   }
+
+  HB_CUDA(cudaEventRecord(ev[2], stream));
 
   // ---- SVD of R_B^T for the sketched blocks ------------------------------------------
   std::vector<JacobiProb> sprobs;
@@ -419,10 +582,33 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     d_sprobs = upload_vec(sprobs, stream);
     jacobi_svd_batched(d_sprobs, (int)sprobs.size(), prm, d_status, max_l, stream);
   }
+  HB_CUDA(cudaEventRecord(ev[3], stream));
   std::vector<int> ints(2 * n_int, 0);
   HB_CUDA(cudaMemcpyAsync(ints.data(), d_int, sizeof(int) * 2 * n_int, cudaMemcpyDeviceToHost,
                           stream));
+  // Frobenius epsilon-rank of every sketched block (for the rank model's
+  // training data): the fewest leading singular values whose discarded tail
+  // has Frobenius norm <= tol * s_0
+  std::vector<int> fro_rank(sk.size(), 0);
+  std::vector<std::vector<double>> core_sig(record ? sk.size() : 0);
+  for (size_t i = 0; i < core_sig.size(); ++i) {
+    core_sig[i].resize(sk[i].ell);
+    HB_CUDA(cudaMemcpyAsync(core_sig[i].data(), sprobs[i].sigma, sizeof(double) * sk[i].ell,
+                            cudaMemcpyDeviceToHost, stream));
+  }
   HB_CUDA(cudaStreamSynchronize(stream));
+  for (size_t i = 0; i < core_sig.size(); ++i) {
+    const std::vector<double> &sv = core_sig[i];
+    if (sv.empty() || !(sv[0] > 0.0)) continue;
+    double tail = 0.0;
+    int r = (int)sv.size();
+    const double lim = tol * sv[0];
+    while (r > 1 && std::sqrt(tail + sv[r - 1] * sv[r - 1]) <= lim) {
+      tail += sv[r - 1] * sv[r - 1];
+      --r;
+    }
+    fro_rank[i] = r;
+  }
   *svd_status = ints[n_int - 1];
   for (auto &B : g.blocks) B.s = 0;
   for (size_t p = 0; p < exact.size(); ++p) g.blocks[exact[p]].s = ints[p];
@@ -467,7 +653,11 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     }
     gemm_f64_run(gf, fb, TileShape::M128N64, stream, false);
   }
+  HB_CUDA(cudaEventRecord(ev[4], stream));
   HB_CUDA(cudaStreamSynchronize(stream));
+  float stage_ms[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
+  for (auto &e : ev) cudaEventDestroy(e);
   dev_free(d_eprobs, stream);
   dev_free(d_sprobs, stream);
   dev_free(d_int, stream);
@@ -495,6 +685,23 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     st.failed_sketch += sw > maxsw;
     st.max_sketch = std::max(st.max_sketch, sk[i].ell);
   }
+  g_last_features.clear();
+  if (record) {
+    for (size_t i = 0; i < sk.size(); ++i) {
+      for (int q = 0; q < kRankIn; ++q) g_last_features.push_back(feats[i * kRankIn + q]);
+      g_last_features.push_back((float)ints[exact.size() + i]);
+      g_last_features.push_back((float)sk[i].pred);
+      g_last_features.push_back((float)sk[i].first_w);
+      g_last_features.push_back(sk[i].fell_back ? 1.f : 0.f);
+      g_last_features.push_back((float)sk[i].ell);
+      g_last_features.push_back((float)fro_rank[i]);
+      st.learned_fallbacks += sk[i].fell_back;
+    }
+  }
+  st.ms_exact = stage_ms[0];
+  st.ms_rounds = stage_ms[1];
+  st.ms_core_svd = stage_ms[2];
+  st.ms_finish = stage_ms[3];
   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   g_last_stats = st;
   if (stats) *stats = st;

@@ -1,6 +1,8 @@
 // Dense -> HODLR construction on the device.
 #pragma once
 
+#include <vector>
+
 #include "dtree.h"
 
 namespace hb {
@@ -14,10 +16,25 @@ struct BuildStats {
   int max_sweeps_exact = 0, max_sweeps_sketch = 0;
   int failed_exact = 0, failed_sketch = 0;
   int max_sketch = 0;          // largest sketch (columns)
+  // device time (ms) of the build's stages, from events on the build stream
+  double ms_exact = 0.0;       // Jacobi SVDs of the small blocks
+  double ms_rounds = 0.0;      // sketch rounds (products, orthonormalisation, decisions)
+  double ms_core_svd = 0.0;    // Jacobi SVDs of the sketched cores R_B^T
+  double ms_finish = 0.0;      // arena, leaf copies, U = Q U_R S, V = P V_R
+  int learned_fallbacks = 0;   // one-shot sketches that failed the error check
 };
 
 // Statistics of the most recent build on the calling thread.
 const BuildStats &last_build_stats();
+
+// Per sketched block of the most recent build that computed features: the 8
+// rank-model features, final rank, predicted rank (-1: no model), first
+// sketch width, fallback flag (1: the one-shot sketch failed its error
+// check), final sketch width, Frobenius epsilon-rank (fewest leading singular
+// values whose discarded tail has Frobenius norm <= tol * s_0; the rank
+// model's training target).
+constexpr int kFeatureRow = 14;
+const std::vector<float> &last_build_features();
 
 // Compresses every off-diagonal block of the n x n matrix d_A (ld lda, device)
 // following the block sizes of `g` (ranks ignored) with hmat_lib's relative

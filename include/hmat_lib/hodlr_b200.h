@@ -87,8 +87,10 @@ int hodlr_b200_kernel_matrix_dev(const double *d_points, int n, int dim, int kin
 int hodlr_b200_phase_times(double *out, int capacity);
 /* Statistics of the calling thread's most recent build: exact blocks,
  * sketched blocks, sketch rounds, seconds, cap hit, max Jacobi sweeps (exact,
- * sketched), unconverged Jacobi problems (exact, sketched), largest sketch.
- * Returns the number of values. */
+ * sketched), unconverged Jacobi problems (exact, sketched), largest sketch,
+ * then the device milliseconds of the stages: small-block SVDs, sketch
+ * rounds, SVDs of the sketched cores, finishing.  Returns the number of
+ * values. */
 int hodlr_b200_build_stats(double *out, int capacity);
 /* y = H x on device buffers, allocating nothing (no counterpart in hmat_lib).
  * For callers that cannot allocate device memory while they run: an
@@ -132,6 +134,49 @@ int hodlr_b200_batched_tuning(char *buf, int capacity);
 int hodlr_b200_batched_check(void);
 /* Drops every cached batched plan (their graphs and scratch). */
 void hodlr_b200_batched_release(void);
+
+/* ---- learned rank predictor (no counterpart in hmat_lib) -------------------
+ * An MLP 8 -> 64 -> 64 -> 1 (ReLU, FP32) maps an off-diagonal block's
+ * features to log2(rank + 1), the rank being the block's Frobenius
+ * epsilon-rank at the build tolerance (the sketch width at which the
+ * randomized range finder's a-posteriori error estimate meets it).  Features: log2(min(m,
+ * n)), depth, ln(kernel length) (option "kernel_length", 0 if unknown),
+ * log10(s_i / s_1) for i = 2, 4, 8, 12, 16 of a 16-column Gaussian sketch of
+ * the block.  Parameters (hodlr_b200_rank_model_size() floats): feature mean
+ * [8], feature scale [8], W1 [8][64], b1 [64], W2 [64][64], b2 [64], W3 [64],
+ * b3.  All arrays below are host memory; the arithmetic runs on the GPU with
+ * the library's own training and inference kernels. */
+int hodlr_b200_rank_model_size(void);
+/* Model used by builds with option "learned_ranks" = 1 (count 0 clears it). */
+int hodlr_b200_rank_model_set(const float *params, int count);
+/* Copies the current model out; returns its size (0: none). */
+int hodlr_b200_rank_model_get(float *params, int capacity);
+/* Trains from scratch on n samples (features n x 8 row-major, targets
+ * log2(rank + 1)) with Adam on mini-batches; writes the parameters and the
+ * full-data loss every 100 steps (up to log_capacity values). */
+int hodlr_b200_rank_model_train(const float *features, const float *targets, int n, int steps,
+                                int batch, double lr, unsigned long long seed, float *params_out,
+                                float *loss_log, int log_capacity);
+/* out[i] = model(params, features[i]). */
+int hodlr_b200_rank_model_predict(const float *params, const float *features, int n,
+                                  float *out);
+/* Mean squared error of the model on n samples and its gradient with respect
+ * to every parameter (the normalisation entries get 0). */
+int hodlr_b200_rank_model_gradient(const float *params, const float *features,
+                                   const float *targets, int n, float *grad_out,
+                                   float *loss_out);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) of step number `step`
+ * (1-based) on the trainable parameters; m and v are updated in place. */
+int hodlr_b200_rank_model_adam(float *params, const float *grad, float *m, float *v, int step,
+                               double lr);
+/* Per sketched block of the calling thread's latest build that computed
+ * features (option "learned_ranks" or "record_features"): 8 features, the
+ * final rank, the predicted rank (-1 without a model), the first sketch
+ * width, whether the block fell back to adaptive growth, the final sketch
+ * width, the Frobenius epsilon-rank (fewest leading singular values whose
+ * discarded tail has Frobenius norm <= tol * s_0).  Rows of 14 floats;
+ * returns the number of rows. */
+int hodlr_b200_build_features(float *out, int capacity_rows);
 
 #ifdef __cplusplus
 }

@@ -136,3 +136,43 @@ def test_oracle_matches_reference_library(seed):
     assert O.rel_fro(td.to_dense(), rd.to_dense()) < 1e-13
     x = rng.standard_normal((n, 4))
     assert O.rel_fro(O.multiply_dense(td, x), ref_lib.multiply_dense(rt, x)) < 1e-13
+
+
+# ---- rank-model oracle (pins oracle/rank_mlp_oracle.py) --------------------------
+
+def test_rank_mlp_oracle_gradient_matches_finite_differences():
+    """Central differences of the oracle's loss against its analytic
+    gradient, on every trainable entry class (W1, b1, W2, b2, W3, b3)."""
+    from oracle import rank_mlp_oracle as R
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((40, R.IN)) * 2.0 + 1.0
+    t = rng.standard_normal(40)
+    p = R.random_params(rng, x)
+    _, g = R.loss_and_gradient(p, x, t)
+    picks = list(rng.choice(np.arange(R.W1, R.B1), 6)) + list(rng.choice(np.arange(R.B1, R.W2), 4)) \
+        + list(rng.choice(np.arange(R.W2, R.B2), 10)) + list(rng.choice(np.arange(R.B2, R.W3), 4)) \
+        + list(rng.choice(np.arange(R.W3, R.B3), 4)) + [R.B3]
+    for i in picks:
+        h = 1e-6
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (R.loss_and_gradient(pp, x, t)[0] - R.loss_and_gradient(pm, x, t)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
+    assert np.all(g[:R.NORM] == 0.0)
+
+
+def test_rank_mlp_oracle_adam_matches_formula():
+    from oracle import rank_mlp_oracle as R
+    rng = np.random.default_rng(4)
+    p = R.random_params(rng)
+    g = rng.standard_normal(R.SIZE)
+    m = np.zeros(R.SIZE)
+    v = np.zeros(R.SIZE)
+    p1, m1, v1 = R.adam_step(p, g, m, v, 1, 1e-2)
+    # first Adam step moves every trainable entry by lr |g| / (|g| + eps)
+    d = (p - p1)[R.NORM:]
+    ga = np.abs(g[R.NORM:])
+    assert np.allclose(np.abs(d), 1e-2 * ga / (ga + 1e-8), rtol=1e-9)
+    assert np.all(np.sign(d) == np.sign(g[R.NORM:]))
+    assert np.array_equal(p1[:R.NORM], p[:R.NORM])

@@ -1,0 +1,208 @@
+"""Learned rank predictor: the library's GPU training and inference kernels
+against the CPU oracle (forward, gradient, Adam step), training on a
+synthetic regression, and the learned build (one-shot sketch sizes from the
+trained network, fallback to the adaptive rule) against the plain build."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from hmat_lib_b200 import abi
+from hmat_lib_b200 import rank_model as RM
+from hmat_lib_b200 import workloads as W
+from hmat_lib_b200.hodlr import DeviceTree
+from oracle import rank_mlp_oracle as R
+from oracle import hodlr_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(n, seed):
+    rng = np.random.default_rng(seed)
+    x = np.column_stack([rng.uniform(7, 14, n), rng.integers(0, 8, n), rng.uniform(-4, -0.7, n),
+                         -rng.uniform(0, 1, n), -rng.uniform(0, 2, n), -rng.uniform(0, 4, n),
+                         -rng.uniform(0, 6, n), -rng.uniform(0, 8, n)]).astype(np.float32)
+    return x, rng
+
+
+def test_forward_matches_oracle():
+    x, rng = _data(1000, 1)
+    p = R.random_params(rng, x.astype(np.float64)).astype(np.float32)
+    got = RM.predict(p, x)
+    want, _ = R.forward(p.astype(np.float64), x.astype(np.float64))
+    assert np.max(np.abs(got - want)) <= 1e-4 * max(1.0, np.max(np.abs(want)))
+
+
+@pytest.mark.parametrize("n", [7, 256, 1000, 4099])
+def test_gradient_matches_oracle(n):
+    """Gradient of the mean squared error from the GPU backward kernels
+    against the oracle's analytic gradient (FP32 vs FP64)."""
+    x, rng = _data(n, n)
+    p = R.random_params(rng, x.astype(np.float64)).astype(np.float32)
+    t = rng.uniform(0, 9, n).astype(np.float32)
+    loss, g = RM.gradient(p, x, t)
+    wl, wg = R.loss_and_gradient(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64))
+    assert abs(loss - wl) <= 1e-4 * wl
+    scale = np.max(np.abs(wg))
+    assert np.max(np.abs(g - wg)) <= 2e-4 * scale
+    assert np.all(g[:R.NORM] == 0.0)
+    # deterministic: the same call gives the same bits
+    _, g2 = RM.gradient(p, x, t)
+    assert np.array_equal(g, g2)
+
+
+def test_adam_matches_oracle():
+    rng = np.random.default_rng(9)
+    p = R.random_params(rng).astype(np.float32)
+    g = rng.standard_normal(R.SIZE).astype(np.float32)
+    m = (rng.standard_normal(R.SIZE) * 0.01).astype(np.float32)
+    v = (rng.random(R.SIZE) * 0.01).astype(np.float32)
+    p1, m1, v1 = RM.adam(p, g, m, v, 7, 3e-3)
+    wp, wm, wv = R.adam_step(p.astype(np.float64), g.astype(np.float64), m.astype(np.float64),
+                             v.astype(np.float64), 7, 3e-3)
+    # FP32 kernel vs FP64 oracle: 1 - 0.999 is 4.7e-5 off in FP32
+    assert np.allclose(p1, wp, rtol=0, atol=1e-6)
+    assert np.allclose(m1, wm, rtol=1e-4, atol=1e-8)
+    assert np.allclose(v1, wv, rtol=1e-4, atol=1e-10)
+
+
+def test_training_fits_a_smooth_target():
+    x, rng = _data(20000, 5)
+    t = (0.5 * x[:, 0] - 0.8 * x[:, 3] * x[:, 1] + np.sin(x[:, 2])).astype(np.float32)
+    p, log = RM.train(x, t, steps=1500, batch=2048, lr=3e-3, seed=2)
+    assert log[-1] < 0.02 * np.var(t)
+    pred = RM.predict(p, x)
+    want, _ = R.forward(p.astype(np.float64), x.astype(np.float64))
+    assert np.max(np.abs(pred - want)) <= 1e-3 * max(1.0, np.max(np.abs(want)))
+
+
+# ---- learned build ----------------------------------------------------------------
+
+KIND = {"gaussian": 0, "matern32": 1, "exponential": 2}
+
+
+def _matrix(n, dim, kind, length, seed):
+    import torch
+    pts = W.points_morton(n, dim, seed) if dim > 1 else W.points_1d_sorted(n, seed)
+    d_pts = torch.from_numpy(np.asfortranarray(pts).T.copy().reshape(-1)).cuda()
+    a = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    assert abi.load().hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, dim,
+                                                   KIND[kind], length, 1e-2,
+                                                   C.c_void_p(a.data_ptr()), n, None) == 0
+    torch.cuda.synchronize()
+    return a
+
+
+def _stats():
+    st = (C.c_double * 15)()
+    abi.load().hodlr_b200_build_stats(st, 15)
+    return dict(rounds=st[2], max_sketch=st[9], fallbacks=st[14])
+
+
+def _build(a, n, h, learned, length):
+    lib = abi.load()
+    lib.hodlr_b200_set_option(b"learned_ranks", 1.0 if learned else 0.0)
+    lib.hodlr_b200_set_option(b"record_features", 1.0)
+    lib.hodlr_b200_set_option(b"kernel_length", length)
+    try:
+        t = DeviceTree.build(a.data_ptr(), n, n, h, 1e-8)
+    finally:
+        lib.hodlr_b200_set_option(b"learned_ranks", 0.0)
+        lib.hodlr_b200_set_option(b"record_features", 0.0)
+        lib.hodlr_b200_set_option(b"kernel_length", 0.0)
+    return t, _stats(), RM.build_features()
+
+
+def _error_vs_dense(a, t, n):
+    import torch
+    x = torch.randn(8, n, dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    t.matmat(x.data_ptr(), 8, n, y.data_ptr(), n)
+    torch.cuda.synchronize()
+    yd = x @ a.view(n, n)
+    return float(torch.linalg.norm(y - yd) / torch.linalg.norm(yd))
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """A model trained in the test on plain builds of 2D Matern / exponential
+    kernels at n = 2048 and 4096 (features and ranks recorded by the build)."""
+    rng = np.random.default_rng(11)
+    xs, ts = [], []
+    for i in range(24):
+        n = int(rng.choice([2048, 4096]))
+        h = (n // 128).bit_length() - 1
+        kind = ["matern32", "exponential"][i % 2]
+        length = float(np.exp(rng.uniform(np.log(0.03), np.log(0.5))))
+        a = _matrix(n, 2, kind, length, 100 + i)
+        t, _, f = _build(a, n, h, False, length)
+        t.free()
+        xs.append(f[:, :8])
+        ts.append(RM.targets_of_ranks(f[:, 13]))
+        del a
+    x = np.concatenate(xs)
+    y = np.concatenate(ts)
+    p, log = RM.train(x, y, steps=2000, batch=1024, lr=3e-3, seed=3)
+    assert log[-1] < 0.5 * np.var(y)
+    RM.set_model(p)
+    yield p
+    RM.set_model(None)
+
+
+def test_learned_build_matches_plain(trained):
+    """Held-out 2D Matern matrix: same ranks within a few, error against the
+    dense product within 1.5x the plain build's, fewer sketch rounds."""
+    n, h, length = 4096, 5, 0.07
+    a = _matrix(n, 2, "matern32", length, 999)
+    tp, sp, fp = _build(a, n, h, False, length)
+    tl, sl, fl = _build(a, n, h, True, length)
+    rp, rl = tp.ranks(), tl.ranks()
+    assert np.max(np.abs(rp - rl)) <= max(3, int(0.03 * rp.max()))
+    ep, el = _error_vs_dense(a, tp, n), _error_vs_dense(a, tl, n)
+    assert el <= 1.5 * ep + 1e-12, (el, ep)
+    assert sl["rounds"] < sp["rounds"]
+    assert np.all(fl[:, 9] >= 1)          # every sketched block got a prediction
+    tp.free()
+    tl.free()
+
+
+def test_fallback_when_prediction_is_too_low(trained):
+    """A model that always predicts rank 1: every larger block fails the
+    one-shot error check and continues with the adaptive rule, ending at the
+    plain build's ranks."""
+    p = np.zeros(R.SIZE, dtype=np.float32)
+    p[R.IN:R.NORM] = 1.0
+    p[R.B3] = 1.0                          # log2(1 + 1)
+    RM.set_model(p)
+    try:
+        n, h, length = 2048, 4, 0.1
+        a = _matrix(n, 2, "matern32", length, 77)
+        tp, sp, _ = _build(a, n, h, False, length)
+        tl, sl, fl = _build(a, n, h, True, length)
+        assert sl["fallbacks"] == np.sum(fl[:, 11] > 0) > 0
+        assert np.max(np.abs(tp.ranks() - tl.ranks())) <= 1
+        assert _error_vs_dense(a, tl, n) <= 1.25 * _error_vs_dense(a, tp, n) + 1e-12
+        tp.free()
+        tl.free()
+    finally:
+        RM.set_model(trained)
+
+
+def test_ablation_learned_vs_plain(trained):
+    """What the network buys: on a held-out exponential-kernel matrix the
+    learned build needs fewer rounds and a smaller largest sketch than the
+    plain adaptive build, at matching accuracy."""
+    n, h, length = 4096, 5, 0.2
+    a = _matrix(n, 2, "exponential", length, 555)
+    tp, sp, fp = _build(a, n, h, False, length)
+    tl, sl, fl = _build(a, n, h, True, length)
+    print("plain rounds", sp["rounds"], "learned rounds", sl["rounds"], "fallbacks", sl["fallbacks"])
+    print("rank / predicted / first width / final width / plain width:")
+    for rp_, rl_ in zip(fp, fl):
+        print(int(rl_[8]), int(rl_[9]), int(rl_[10]), int(rl_[12]), int(rp_[12]))
+    assert sl["rounds"] < sp["rounds"]
+    # the core SVD costs ~ sum of (sketch width)^3
+    assert np.sum(fl[:, 12].astype(np.float64) ** 3) < np.sum(fp[:, 12].astype(np.float64) ** 3)
+    assert _error_vs_dense(a, tl, n) <= 1.5 * _error_vs_dense(a, tp, n) + 1e-12
+    tp.free()
+    tl.free()
