@@ -169,6 +169,15 @@ def run_cpu_baseline(n: int, k: int):
         return {"error": str(e)[:200]}
 
 
+def build_stats(lib):
+    """Stage times and counters of the calling thread's latest build."""
+    st = (C.c_double * 15)()
+    lib.hodlr_b200_build_stats(st, 15)
+    return {"sketched_blocks": int(st[1]), "sketch_rounds": int(st[2]),
+            "largest_sketch": int(st[9]), "ms_small_svd": st[10], "ms_rounds": st[11],
+            "ms_core_svd": st[12], "ms_finish": st[13], "learned_fallbacks": int(st[14])}
+
+
 def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream):
     """The uneven batch: `count` HODLRs (n in {1024, 2048, 4096, 8192},
     exponential kernel on sorted 1D points, leaf 128, tol 1e-8), each times a
@@ -344,6 +353,25 @@ def main():
         build_s = time.perf_counter() - t0
     info = tree.info()
     ranks = tree.ranks()
+    plain_stats = build_stats(lib)
+
+    # ---- learned build: sketches sized in one shot by the shipped rank model ------
+    from hmat_lib_b200 import rank_model as RM
+    RM.load_default()
+    lib.hodlr_b200_set_option(b"learned_ranks", 1.0)
+    lib.hodlr_b200_set_option(b"kernel_length", w["length"])
+    try:
+        with torch.cuda.stream(stream):
+            stream.synchronize()
+            t0 = time.perf_counter()
+            tree_l = DeviceTree.build(a.data_ptr(), n, n, h, tol, stream=sh)
+            stream.synchronize()
+            build_s_learned = time.perf_counter() - t0
+    finally:
+        lib.hodlr_b200_set_option(b"learned_ranks", 0.0)
+        lib.hodlr_b200_set_option(b"kernel_length", 0.0)
+    learned_stats = build_stats(lib)
+    ranks_l = tree_l.ranks()
 
     # ---- accuracy against the dense FP64 product (checker: cuBLAS on A) ------------
     x = torch.randn(k, n, dtype=torch.float64, device=dev)      # column-major n x k
@@ -353,6 +381,12 @@ def main():
     a_mat = a.view(n, n)          # row-major view of column-major A = A^T
     y_dense = (x @ a_mat)         # (k x n) = (A X)^T in column-major terms
     rel_err = (torch.linalg.norm(y - y_dense) / torch.linalg.norm(y_dense)).item()
+    y_l = torch.zeros(k, n, dtype=torch.float64, device=dev)
+    tree_l.matmat(x.data_ptr(), k, n, y_l.data_ptr(), n, stream=sh)
+    stream.synchronize()
+    rel_err_learned = (torch.linalg.norm(y_l - y_dense) / torch.linalg.norm(y_dense)).item()
+    del y_l
+    tree_l.free()
     del a, a_mat, y_dense
     torch.cuda.empty_cache()
 
@@ -493,6 +527,13 @@ def main():
                    "l2": "inputs larger than L2 (factors + X > 126 MB), no flush",
                    "parallelism": f"replicas{world}"},
         "build_s": build_s,
+        "build": {"plain": dict(seconds=build_s, rel_err_vs_dense=rel_err, **plain_stats),
+                  "learned": dict(seconds=build_s_learned, rel_err_vs_dense=rel_err_learned,
+                                  max_rank_diff_vs_plain=int(np.max(np.abs(ranks_l - ranks))),
+                                  **learned_stats),
+                  "speedup_learned_vs_plain": build_s / build_s_learned,
+                  "model": "hmat_lib_b200/rank_model.f32 (MLP 8-64-64-1, trained by the "
+                           "library's GPU kernels)"},
         "rel_err_vs_dense": rel_err,
         "rel_err_mixed_vs_fp64": rel_err_mixed_vs_fp64,
         "tree": {"max_rank": info["max_rank"], "storage_doubles": storage,
