@@ -1,24 +1,30 @@
-// Batched one-sided (Hestenes) Jacobi SVD in FP64, one CTA per problem.
+// Batched one-sided (Hestenes) Jacobi SVD in FP64, one CTA per problem, or a
+// cluster of CTAs per wide problem.
 //
 // Replaces the LAPACK dgesdd calls of hmat_lib (src/lapack_wrapper.c:8-59
 // via src/constructors.c:323 for compression; src/hodlr_algebra.c:153 and
 // :301 for recompression) on blocks small enough for one CTA.  Columns of the
 // tall orientation are orthogonalised pairwise in round-robin order: each
 // round pairs every column with one other (C/2 disjoint pairs, one warp per
-// pair), so a sweep is C-1 rounds separated by __syncthreads.  The singular
+// pair), so a sweep is C-1 rounds separated by barriers.  The singular
 // values come out with high relative accuracy, so the relative truncation
 // rule picks the same rank as the reference's dgesdd on its test matrices.
 // Every loop is bounded: a problem that has not converged after max_sweeps
 // sweeps still writes its outputs and raises SVD_FAILURE in the status word.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "jacobi.h"
+
+namespace cg = cooperative_groups;
 
 namespace hb {
 
 namespace {
 
 constexpr int kJThreads = 256;
+constexpr int kJCluster = 8;        // CTAs per problem cluster
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -26,9 +32,39 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-__global__ void __launch_bounds__(kJThreads)
-jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *status) {
-  const JacobiProb P = probs[blockIdx.x];
+// Global loads and stores of G and W.  A problem solved by a cluster of CTAs
+// reads columns that other CTAs of the cluster rotated in the previous round,
+// so it bypasses L1 (cache-global) and relies on the cluster barrier's
+// release / acquire ordering at L2.
+template <bool kTeam>
+__device__ __forceinline__ double gld(const double *p) {
+  if constexpr (kTeam) return __ldcg(p);
+  return *p;
+}
+template <bool kTeam>
+__device__ __forceinline__ void gst(double *p, double v) {
+  if constexpr (kTeam)
+    __stcg(p, v);
+  else
+    *p = v;
+}
+
+template <bool kTeam>
+__device__ __forceinline__ void team_sync() {
+  if constexpr (kTeam)
+    cg::this_cluster().sync();
+  else
+    __syncthreads();
+}
+
+// One problem, by one CTA (kTeam false) or by the kJCluster CTAs of a
+// cluster (kTeam true, `crank` = this CTA's rank in it): the disjoint pairs
+// of a round are spread over every warp of the team, rounds are separated by
+// a barrier of the team, and the team agrees on convergence through the
+// CTAs' shared memory.  Every pair's arithmetic is the same in both modes.
+template <bool kTeam>
+__device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *status,
+                             int crank, int team) {
   const int m = P.m, n = P.n;
   const bool tall = m >= n;
   const int R = tall ? m : n, C = tall ? n : m;
@@ -37,32 +73,31 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
   double *s_sig = sh;                              // C
   int *s_perm = reinterpret_cast<int *>(sh + C);   // C
   __shared__ double s_off[32];
+  __shared__ double s_team_off;
 
-  if (C == 0) {
-    if (tid == 0 && P.rank) *P.rank = 0;
-    return;
-  }
   double *G = P.G, *W = P.W;
-  for (long long e = tid; e < (long long)R * C; e += blockDim.x) {
+  const int gtid = crank * blockDim.x + tid, gthreads = team * blockDim.x;
+  for (long long e = gtid; e < (long long)R * C; e += gthreads) {
     const int r = (int)(e % R), c = (int)(e / R);
     // logical element (i, j) of the m x n input
     const int i = tall ? r : c, j = tall ? c : r;
-    G[e] = P.transA ? P.A[j + (long long)i * P.lda] : P.A[i + (long long)j * P.lda];
+    gst<kTeam>(G + e, P.transA ? P.A[j + (long long)i * P.lda] : P.A[i + (long long)j * P.lda]);
   }
-  for (long long e = tid; e < (long long)C * C; e += blockDim.x)
-    W[e] = ((e % C) == (e / C)) ? 1.0 : 0.0;
-  __syncthreads();
+  for (long long e = gtid; e < (long long)C * C; e += gthreads)
+    gst<kTeam>(W + e, ((e % C) == (e / C)) ? 1.0 : 0.0);
+  team_sync<kTeam>();
 
   // a computed dot product of length R carries ~sqrt(R) eps relative noise:
   // below that no rotation can make progress
   const double conv = fmax(prm.conv_tol, 4.0 * sqrt((double)R) * 2.220446049250313e-16);
   const int players = C + (C & 1);
+  const int gwarp = crank * nwarps + warp, gwarps = team * nwarps;
   int sweep = 0;
   bool converged = (C == 1);
   for (; sweep < prm.max_sweeps && !converged; ++sweep) {
     double off = 0.0;
     for (int r = 0; r < players - 1; ++r) {
-      for (int k = warp; k < players / 2; k += nwarps) {
+      for (int k = gwarp; k < players / 2; k += gwarps) {
         int a, b;
         if (k == 0) {
           a = r;
@@ -76,7 +111,7 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
         double *gp = G + (long long)p * R, *gq = G + (long long)q * R;
         double al = 0.0, be = 0.0, ga = 0.0;
         for (int i = lane; i < R; i += 32) {
-          const double x = gp[i], y = gq[i];
+          const double x = gld<kTeam>(gp + i), y = gld<kTeam>(gq + i);
           al = fma(x, x, al);
           be = fma(y, y, be);
           ga = fma(x, y, ga);
@@ -96,29 +131,41 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
                              : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
         const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
         for (int i = lane; i < R; i += 32) {
-          const double x = gp[i], y = gq[i];
-          gp[i] = cs * x - sn * y;
-          gq[i] = sn * x + cs * y;
+          const double x = gld<kTeam>(gp + i), y = gld<kTeam>(gq + i);
+          gst<kTeam>(gp + i, cs * x - sn * y);
+          gst<kTeam>(gq + i, sn * x + cs * y);
         }
         double *wp = W + (long long)p * C, *wq = W + (long long)q * C;
         for (int i = lane; i < C; i += 32) {
-          const double x = wp[i], y = wq[i];
-          wp[i] = cs * x - sn * y;
-          wq[i] = sn * x + cs * y;
+          const double x = gld<kTeam>(wp + i), y = gld<kTeam>(wq + i);
+          gst<kTeam>(wp + i, cs * x - sn * y);
+          gst<kTeam>(wq + i, sn * x + cs * y);
         }
       }
-      __syncthreads();
+      team_sync<kTeam>();
     }
-    // block-wide max of `off`
+    // team-wide max of `off`
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) off = fmax(off, __shfl_xor_sync(0xffffffffu, off, o));
     if (lane == 0) s_off[warp] = off;
     __syncthreads();
     double mx = 0.0;
     for (int w = 0; w < nwarps; ++w) mx = fmax(mx, s_off[w]);
+    if constexpr (kTeam) {
+      // every CTA reads every CTA's maximum, so all take the same decision;
+      // the second barrier keeps every CTA (and its shared memory) alive and
+      // unchanged until all reads are done
+      cg::cluster_group cl = cg::this_cluster();
+      if (tid == 0) s_team_off = mx;
+      cl.sync();
+      mx = 0.0;
+      for (int rk = 0; rk < team; ++rk) mx = fmax(mx, *cl.map_shared_rank(&s_team_off, rk));
+      cl.sync();
+    }
     converged = mx <= conv;
     __syncthreads();
   }
+  if (crank != 0) return;
   if (!converged && tid == 0) atomicExch(status, (int)SVD_FAILURE);
   if (tid == 0 && P.sweeps) *P.sweeps = converged ? sweep : prm.max_sweeps + 1;
 
@@ -126,7 +173,10 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
   for (int j = warp; j < C; j += nwarps) {
     const double *gj = G + (long long)j * R;
     double s = 0.0;
-    for (int i = lane; i < R; i += 32) s = fma(gj[i], gj[i], s);
+    for (int i = lane; i < R; i += 32) {
+      const double x = gld<kTeam>(gj + i);
+      s = fma(x, x, s);
+    }
     s = warp_sum(s);
     if (lane == 0) s_sig[j] = sqrt(s);
   }
@@ -167,15 +217,54 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
     double *v = P.V + (long long)k * P.ldv;
     if (tall) {  // A = (G / sigma) Sigma W^T
       for (int i = lane; i < m; i += 32) {
-        double x = gj[i];
+        double x = gld<kTeam>(gj + i);
         if (!prm.scale_u) x = sg > 0.0 ? x / sg : (i == k % m ? 1.0 : 0.0);
         u[i] = x;
       }
-      for (int i = lane; i < n; i += 32) v[i] = wj[i];
+      for (int i = lane; i < n; i += 32) v[i] = gld<kTeam>(wj + i);
     } else {     // A^T = (G / sigma) Sigma W^T  =>  A = W Sigma (G / sigma)^T
-      for (int i = lane; i < m; i += 32) u[i] = prm.scale_u ? wj[i] * sg : wj[i];
-      for (int i = lane; i < n; i += 32) v[i] = sg > 0.0 ? gj[i] / sg : (i == k % n ? 1.0 : 0.0);
+      for (int i = lane; i < m; i += 32) {
+        const double x = gld<kTeam>(wj + i);
+        u[i] = prm.scale_u ? x * sg : x;
+      }
+      for (int i = lane; i < n; i += 32) {
+        const double x = gld<kTeam>(gj + i);
+        v[i] = sg > 0.0 ? x / sg : (i == k % n ? 1.0 : 0.0);
+      }
     }
+  }
+}
+
+// One CTA per problem.
+__global__ void __launch_bounds__(kJThreads)
+jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *status) {
+  const JacobiProb P = probs[blockIdx.x];
+  const int C = P.m < P.n ? P.m : P.n;
+  if (C == 0) {
+    if (threadIdx.x == 0 && P.rank) *P.rank = 0;
+    return;
+  }
+  jacobi_solve<false>(P, prm, status, 0, 1);
+}
+
+// A cluster of kJCluster CTAs per problem; problems with at least
+// `team_min_c` columns are solved by the whole cluster, the others by its
+// first CTA alone (the rest return at once, before any cluster barrier).
+__global__ void __cluster_dims__(kJCluster, 1, 1) __launch_bounds__(kJThreads)
+jacobi_svd_cluster_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *status,
+                          int team_min_c) {
+  const int crank = (int)cg::this_cluster().block_rank();
+  const JacobiProb P = probs[blockIdx.x / kJCluster];
+  const int C = P.m < P.n ? P.m : P.n;
+  if (C == 0) {
+    if (crank == 0 && threadIdx.x == 0 && P.rank) *P.rank = 0;
+    return;
+  }
+  if (C >= team_min_c) {
+    jacobi_solve<true>(P, prm, status, crank, kJCluster);
+  } else {
+    if (crank != 0) return;
+    jacobi_solve<false>(P, prm, status, 0, 1);
   }
 }
 
@@ -206,10 +295,21 @@ void jacobi_svd_batched(const JacobiProb *d_probs, int nprobs, const JacobiParam
   if (nprobs <= 0) return;
   const size_t smem = (size_t)std::max(max_c, 1) * (sizeof(double) + sizeof(int));
   HB_REQUIRE(smem <= 200 * 1024, INPUT_ERROR, "Jacobi SVD problem too wide for one CTA");
-  if (smem > 48 * 1024)
-    HB_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-  jacobi_svd_kernel<<<nprobs, kJThreads, smem, stream>>>(d_probs, prm, d_status);
+  // launches whose widest problem reaches team_min_c columns give every
+  // problem a cluster of CTAs; the others one CTA
+  const int team_min_c = (int)std::min(option("jacobi_cluster_min_c", 192.0), 1e9);
+  if (max_c >= team_min_c) {
+    if (smem > 48 * 1024)
+      HB_CUDA(cudaFuncSetAttribute(jacobi_svd_cluster_kernel,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    jacobi_svd_cluster_kernel<<<nprobs * kJCluster, kJThreads, smem, stream>>>(d_probs, prm,
+                                                                            d_status, team_min_c);
+  } else {
+    if (smem > 48 * 1024)
+      HB_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    jacobi_svd_kernel<<<nprobs, kJThreads, smem, stream>>>(d_probs, prm, d_status);
+  }
   HB_LAUNCHED();
 }
 
