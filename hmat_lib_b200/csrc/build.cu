@@ -63,9 +63,9 @@ thread_local std::vector<float> g_last_features;
 constexpr int kFeatCols = 16;   // width of the feature sketch
 
 // Rank-model features of every sketched block (rank_mlp.h): a 16-column
-// Gaussian sketch Y = A_b Omega, its singular values by the batched Jacobi
-// SVD, then log block size, depth, ln(kernel length) and five log ratios of
-// the sketch's singular values.
+// Gaussian sketch Y = A_b Omega, its R factor by TSQR and the singular values
+// of R (= those of Y) by the batched Jacobi SVD, then log block size, depth,
+// ln(kernel length) and five log ratios of the sketch's singular values.
 std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlock> &sk,
                                   const double *d_A, long long lda, unsigned long long seed,
                                   cudaStream_t stream) {
@@ -73,28 +73,31 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
   std::vector<float> f((size_t)nsk * kRankIn, 0.f);
   if (nsk == 0) return f;
   long long total = 0;
-  std::vector<long long> om(nsk), y(nsk), ws(nsk), u(nsk), v(nsk), sg(nsk);
+  constexpr int F = kFeatCols;
+  std::vector<long long> om(nsk), y(nsk), r(nsk), ws(nsk), u(nsk), v(nsk), sg(nsk);
+  auto take = [&](long long e) {
+    const long long o = total;
+    total += align_up(std::max<long long>(e, 1));
+    return o;
+  };
   for (int i = 0; i < nsk; ++i) {
     const SketchBlock &S = sk[i];
-    auto take = [&](long long e) {
-      const long long o = total;
-      total += align_up(std::max<long long>(e, 1));
-      return o;
-    };
-    om[i] = take((long long)S.n * kFeatCols);
-    y[i] = take((long long)S.m * kFeatCols);
-    ws[i] = take(jacobi_workspace(S.m, kFeatCols));
-    u[i] = take((long long)S.m * kFeatCols);
-    v[i] = take(kFeatCols * kFeatCols);
-    sg[i] = take(kFeatCols);
+    om[i] = take((long long)S.n * F);
+    y[i] = take((long long)S.m * F);
+    r[i] = take(F * F);
+    ws[i] = take(jacobi_workspace(F, F));
+    u[i] = take(F * F);
+    v[i] = take(F * F);
+    sg[i] = take(F);
   }
   double *w = dev_alloc(total, stream);
+  HB_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * total, stream));
   int *d_rank = nullptr;
   HB_CUDA(cudaMallocAsync((void **)&d_rank, sizeof(int) * (nsk + 1), stream));
   HB_CUDA(cudaMemsetAsync(d_rank, 0, sizeof(int) * (nsk + 1), stream));
   std::vector<RandDesc> rd;
   for (int i = 0; i < nsk; ++i)
-    rd.push_back(RandDesc{w + om[i], sk[i].n, sk[i].n, kFeatCols,
+    rd.push_back(RandDesc{w + om[i], sk[i].n, sk[i].n, F,
                           (1ULL << 60) + ((unsigned long long)sk[i].b << 8)});
   gaussian_fill(rd, seed, stream);
   GemmBases bases{};
@@ -103,24 +106,35 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
   GemmBatch gb;
   for (int i = 0; i < nsk; ++i) {
     const SketchBlock &S = sk[i];
-    int pr = gb.add(1, y[i], S.m, S.m, kFeatCols);
+    int pr = gb.add(1, y[i], S.m, S.m, F);
     gb.seg(pr, 0, S.a_off, lda, 0, 1, om[i], S.n, 0, S.n);
   }
   gemm_f64_run(gb, bases, TileShape::M128N64, stream);
+  std::vector<TsqrProb> tp;
+  for (int i = 0; i < nsk; ++i) {
+    TsqrProb t;
+    t.Y = w + y[i];
+    t.ldy = sk[i].m;
+    t.m = sk[i].m;
+    t.w = F;
+    t.R = w + r[i];
+    t.ldr = F;
+    tp.push_back(t);
+  }
+  tsqr_batched(tp, stream);
   std::vector<JacobiProb> jp;
   for (int i = 0; i < nsk; ++i) {
-    const SketchBlock &S = sk[i];
     JacobiProb q{};
-    q.A = w + y[i];
-    q.lda = S.m;
-    q.m = S.m;
-    q.n = kFeatCols;
+    q.A = w + r[i];
+    q.lda = F;
+    q.m = F;
+    q.n = F;
     q.G = w + ws[i];
-    q.W = q.G + align_up((long long)S.m * kFeatCols);
+    q.W = q.G + align_up(F * F);
     q.U = w + u[i];
-    q.ldu = S.m;
+    q.ldu = F;
     q.V = w + v[i];
-    q.ldv = kFeatCols;
+    q.ldv = F;
     q.sigma = w + sg[i];
     q.rank = d_rank + i;
     jp.push_back(q);
@@ -129,10 +143,10 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
   prm.trunc = Truncation::None;
   prm.max_sweeps = 30;
   JacobiProb *d_jp = upload_vec(jp, stream);
-  jacobi_svd_batched(d_jp, nsk, prm, d_rank + nsk, kFeatCols, stream);
-  std::vector<double> sig((size_t)nsk * kFeatCols);
+  jacobi_svd_batched(d_jp, nsk, prm, d_rank + nsk, F, stream);
+  std::vector<double> sig((size_t)nsk * F);
   for (int i = 0; i < nsk; ++i)
-    HB_CUDA(cudaMemcpyAsync(&sig[(size_t)i * kFeatCols], w + sg[i], sizeof(double) * kFeatCols,
+    HB_CUDA(cudaMemcpyAsync(&sig[(size_t)i * F], w + sg[i], sizeof(double) * F,
                             cudaMemcpyDeviceToHost, stream));
   HB_CUDA(cudaStreamSynchronize(stream));
   cudaFreeAsync(d_jp, stream);
@@ -145,16 +159,15 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
     row[0] = (float)std::log2((double)std::min(S.m, S.n));
     row[1] = (float)g.blocks[S.b].depth;
     row[2] = length > 0.0 ? (float)std::log(length) : 0.f;
-    const double *sv = &sig[(size_t)i * kFeatCols];
+    const double *sv = &sig[(size_t)i * F];
     const int idx[5] = {1, 3, 7, 11, 15};   // s_2, s_4, s_8, s_12, s_16
     for (int q = 0; q < 5; ++q) {
-      const double r = sv[0] > 0.0 ? sv[idx[q]] / sv[0] : 0.0;
-      row[3 + q] = (float)std::max(-20.0, r > 0.0 ? std::log10(r) : -20.0);
+      const double rr = sv[0] > 0.0 ? sv[idx[q]] / sv[0] : 0.0;
+      row[3 + q] = (float)std::max(-20.0, rr > 0.0 ? std::log10(rr) : -20.0);
     }
   }
   return f;
 }
-
 }  // namespace
 
 const BuildStats &last_build_stats() { return g_last_stats; }
@@ -222,6 +235,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   std::vector<float> model;
   const bool have_model = learned && rank_model(model);
   for (SketchBlock &S : sk) S.first_w = std::min(w_first, S.cap);
+  const auto tf0 = std::chrono::steady_clock::now();
   if (record && !sk.empty()) {
     feats = block_features(g, sk, d_A, lda, seed, stream);
     if (have_model) {
@@ -268,6 +282,8 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     S.c = take((long long)S.cap * kPanel);
     S.rn = take((long long)kPanel * kPanel + kPanel + wb);
   }
+  const double ms_features =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tf0).count();
   const double eta_learned = option("learned_eta", 1.0);
 
   double *work = dev_alloc(scratch, stream);
@@ -698,6 +714,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
       st.learned_fallbacks += sk[i].fell_back;
     }
   }
+  st.ms_features = ms_features;
   st.ms_exact = stage_ms[0];
   st.ms_rounds = stage_ms[1];
   st.ms_core_svd = stage_ms[2];

@@ -22,6 +22,7 @@ struct BuildStats {
   double ms_core_svd = 0.0;    // Jacobi SVDs of the sketched cores R_B^T
   double ms_finish = 0.0;      // arena, leaf copies, U = Q U_R S, V = P V_R
   int learned_fallbacks = 0;   // one-shot sketches that failed the error check
+  double ms_features = 0.0;    // rank-model features and prediction (host clock)
 };
 
 // Statistics of the most recent build on the calling thread.

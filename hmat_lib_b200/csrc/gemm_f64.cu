@@ -232,11 +232,15 @@ void launch_gemm(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stre
 }  // namespace
 
 GemmPlan::~GemmPlan() {
-  if (dev) cudaFree(dev);
+  if (!dev) return;
+  if (transient)
+    cudaFreeAsync(dev, stream);
+  else
+    cudaFree(dev);
 }
 
 void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool allow_split,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, bool transient) {
   const int BM = tile_rows(shape);
   const int BN = tile_cols(shape);
   plan.shape = shape;
@@ -298,10 +302,18 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
   const size_t bt = tiles.size() * sizeof(GemmTile);
   const size_t total = align_up(bs, 256) + align_up(bp, 256) + align_up(bt, 256) + 256;
   if (plan.dev) {
-    cudaFree(plan.dev);
+    if (plan.transient)
+      cudaFreeAsync(plan.dev, plan.stream);
+    else
+      cudaFree(plan.dev);
     plan.dev = nullptr;
   }
-  HB_CUDA(cudaMalloc(&plan.dev, total));
+  plan.transient = transient;
+  plan.stream = stream;
+  if (transient)
+    HB_CUDA(cudaMallocAsync(&plan.dev, total, stream));
+  else
+    HB_CUDA(cudaMalloc(&plan.dev, total));
   char *base = (char *)plan.dev;
   plan.segs = (GemmSeg *)base;
   plan.probs = (GemmProb *)(base + align_up(bs, 256));
@@ -310,9 +322,10 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
   if (bs) std::memcpy(host.data(), batch.segs.data(), bs);
   if (bp) std::memcpy(host.data() + align_up(bs, 256), probs.data(), bp);
   if (bt) std::memcpy(host.data() + align_up(bs, 256) + align_up(bp, 256), tiles.data(), bt);
-  // pageable source: staged by the driver before the call returns
+  // pageable source: staged by the driver before the call returns, so the
+  // host buffer may go away at once
   HB_CUDA(cudaMemcpyAsync(plan.dev, host.data(), total, cudaMemcpyHostToDevice, stream));
-  HB_CUDA(cudaStreamSynchronize(stream));
+  if (!transient) HB_CUDA(cudaStreamSynchronize(stream));
 }
 
 void gemm_plan_run(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stream) {
@@ -334,9 +347,8 @@ void gemm_f64_run(GemmBatch &batch, const GemmBases &bases, TileShape shape, cud
                   bool allow_split) {
   if (batch.empty()) return;
   GemmPlan plan;
-  gemm_plan_build(plan, batch, shape, allow_split, stream);
+  gemm_plan_build(plan, batch, shape, allow_split, stream, true);
   gemm_plan_run(plan, bases, stream);
-  HB_CUDA(cudaStreamSynchronize(stream));
 }
 
 }  // namespace hb

@@ -92,6 +92,8 @@ struct GemmPlan {
   int nprobs = 0;
   bool any_split = false;
   void *dev = nullptr;          // one allocation holding the three arrays
+  bool transient = false;       // dev is stream-ordered (freed with cudaFreeAsync on `stream`)
+  cudaStream_t stream = nullptr;
   GemmSeg *segs = nullptr;
   GemmProb *probs = nullptr;
   GemmTile *tiles = nullptr;
@@ -102,9 +104,11 @@ struct GemmPlan {
 };
 
 // Builds the tile list (splitting long K ranges when the batch would not
-// fill the GPU) and uploads it.
+// fill the GPU) and uploads it.  A transient plan lives in stream-ordered
+// memory of `stream` and is released in stream order: no host
+// synchronisation.
 void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool allow_split,
-                     cudaStream_t stream);
+                     cudaStream_t stream, bool transient = false);
 
 // Launches a plan: the beta pre-pass for split problems, then the GEMM.
 void gemm_plan_run(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stream);
