@@ -24,10 +24,13 @@ void set_last_error(const std::string &msg);
 void set_last_error_static(const char *msg);
 const char *last_error();
 
+// A failed runtime call also becomes the thread's "last error"; it is read
+// back here so that a later launch check does not report it a second time.
 #define HB_CUDA(call)                                                        \
   do {                                                                       \
     cudaError_t e_ = (call);                                                 \
     if (e_ != cudaSuccess) {                                                 \
+      (void)cudaGetLastError();                                              \
       throw ::hb::Error{ALLOCATION_FAILURE,                                  \
                         std::string(#call) + ": " + cudaGetErrorString(e_)}; \
     }                                                                        \

@@ -4,7 +4,7 @@
 
 Every draw is a seeded kernel matrix (exponential or Matern-3/2 kernel with
 length l ~ logU[0.02, 0.5] plus 1e-2 I, on 1D sorted, 2D or 3D Morton-ordered
-points, n in 2048..16384, leaf 128) generated on the device and compressed
+points, n in 2048..65536, leaf 128) generated on the device and compressed
 by the plain adaptive build at tol 1e-8 with feature recording on: each
 sketched block contributes its 8 features and its Frobenius epsilon-rank
 (the training target, as log2(rank + 1)).  The network is then trained by
@@ -39,7 +39,8 @@ def draws(count: int, seed: int):
             kind=str(rng.choice(["exponential", "matern32"])),
             dim=int(rng.choice([1, 2, 3], p=[0.1, 0.5, 0.4])),
             length=float(math.exp(rng.uniform(math.log(0.02), math.log(0.5)))),
-            n=int(rng.choice([2048, 4096, 8192, 16384], p=[0.35, 0.35, 0.2, 0.1])),
+            n=int(rng.choice([2048, 4096, 8192, 16384, 32768, 65536],
+                             p=[0.25, 0.25, 0.2, 0.17, 0.1, 0.03])),
             seed=int(seed * 100000 + i)))
     return out
 
@@ -54,7 +55,7 @@ def collect(specs, max_seconds: float):
     import torch
     lib = abi.load()
     lib.hodlr_b200_set_option(b"record_features", 1.0)
-    rows, owner, skipped, t0 = [], [], 0, time.perf_counter()
+    rows, owner, skipped, failed, t0 = [], [], 0, 0, time.perf_counter()
     nmax = max(d["n"] for d in specs)
     a = torch.empty(nmax * nmax, dtype=torch.float64, device="cuda")
     try:
@@ -65,16 +66,26 @@ def collect(specs, max_seconds: float):
             pts = W.points_morton(n, dim, d["seed"]) if dim > 1 else \
                 W.points_1d_sorted(n, d["seed"])
             d_pts = torch.from_numpy(np.asfortranarray(pts).T.copy().reshape(-1)).cuda()
-            assert lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, dim,
-                                                    KIND[d["kind"]], d["length"], 1e-2,
-                                                    C.c_void_p(a.data_ptr()), n, None) == 0
+            if lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, dim,
+                                                KIND[d["kind"]], d["length"], 1e-2,
+                                                C.c_void_p(a.data_ptr()), n, None) != 0:
+                failed += 1
+                print(f"draw {i}: kernel matrix failed: "
+                      f"{lib.hodlr_b200_last_error().decode()}", flush=True)
+                continue
             lib.hodlr_b200_set_option(b"kernel_length", d["length"])
             h = (n // 128).bit_length() - 1
             try:
                 t = DeviceTree.build(a.data_ptr(), n, n, h, 1e-8)
-            except HodlrError:
-                skipped += 1          # a block reached the sketch cap: no label
+            except HodlrError as e:
+                # a block reached the sketch cap (no label), or the build ran
+                # out of memory
+                skipped += 1
+                if e.code != abi.SVD_FAILURE:
+                    print(f"draw {i}: build failed: {e}", flush=True)
                 continue
+            if (i + 1) % 100 == 0:
+                print(f"{i + 1} draws, {time.perf_counter() - t0:.0f} s", flush=True)
             f = RM.build_features()
             t.free()
             rows.append(f)
@@ -83,7 +94,7 @@ def collect(specs, max_seconds: float):
         lib.hodlr_b200_set_option(b"record_features", 0.0)
         lib.hodlr_b200_set_option(b"kernel_length", 0.0)
     data = np.concatenate(rows) if rows else np.zeros((0, RM.FEATURE_ROW), np.float32)
-    return data, np.array(owner), skipped, len(rows), time.perf_counter() - t0
+    return data, np.array(owner), skipped + failed, len(rows), time.perf_counter() - t0
 
 
 def main():
@@ -109,7 +120,7 @@ def main():
     p, log = RM.train(x[train], target[train], steps=args.steps, batch=args.batch, lr=args.lr,
                       seed=args.seed)
     train_s = time.perf_counter() - t0
-    summary = dict(draws_requested=args.draws, draws_used=used, draws_skipped_cap=skipped,
+    summary = dict(draws_requested=args.draws, draws_used=used, draws_skipped=skipped,
                    collect_seconds=secs, samples=int(len(x)), train_samples=int(train.sum()),
                    holdout_samples=int(hold.sum()), steps=args.steps, batch=args.batch,
                    lr=args.lr, train_seconds=train_s, loss_every_100_steps=[float(v) for v in log])
