@@ -180,6 +180,11 @@ class DeviceTree:
             msp = C.cast(arr, abi.IP)
         lib().hodlr_b200_build_dev(height, n, msp, C.c_void_p(d_matrix_ptr), ld, tol, 0,
                                    C.c_void_p(stream), C.byref(out), C.byref(ierr))
+        if ierr.value != abi.SUCCESS and out.value:
+            # a failed build still hands over the tree it made: release it
+            msg = lib().hodlr_b200_last_error().decode()
+            lib().hodlr_b200_tree_free(out)
+            raise HodlrError(ierr.value, "hodlr_b200_build_dev", msg)
         _check(ierr, "hodlr_b200_build_dev")
         return cls(out)
 

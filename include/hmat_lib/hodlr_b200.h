@@ -49,7 +49,10 @@ long long hodlr_b200_kernel_launches(void);
 
 /* Build from a device-resident n x n column-major matrix (leading dimension
  * ld), block sizes halved as dense_to_tree_hodlr does (ms == NULL) or given
- * per leaf (2^height entries).  flags: 0. */
+ * per leaf (2^height entries).  flags: 0.  Like dense_to_tree_hodlr, a build
+ * that ends with SVD_FAILURE (a Jacobi SVD out of sweeps, or a rank at the
+ * sketch cap) still stores the tree it made in *out: the caller frees it with
+ * hodlr_b200_tree_free.  Other errors leave *out untouched. */
 int hodlr_b200_build_dev(int height, int n, const int *ms, const double *d_matrix, int ld,
                          double svd_threshold, int flags, void *stream, hodlr_b200_tree *out,
                          int *ierr);

@@ -9,7 +9,7 @@ import pytest
 
 from hmat_lib_b200 import abi
 from hmat_lib_b200 import workloads as W
-from hmat_lib_b200.hodlr import Tree, HodlrError
+from hmat_lib_b200.hodlr import DeviceTree, Tree, HodlrError
 from oracle import hodlr_oracle as O
 
 import cases as K
@@ -164,3 +164,30 @@ def test_sketched_build_2d_matern(n, h):
     assert O.rel_fro(t.matmat(x), a @ x) <= 1.25 * O.rel_fro(yo, a @ x) + 1e-12
     assert O.rel_fro(t.matmat(x), yo) < 2e-8
     t.free()
+
+
+def test_failed_device_builds_release_their_trees(lib):
+    """A device build that ends with SVD_FAILURE hands its tree to the caller
+    (as dense_to_tree_hodlr does); the Python wrapper frees it before raising,
+    so repeated failures do not grow device memory."""
+    import torch
+    n = 4096
+    pts = W.points_morton(n, 2, seed=3)
+    a = torch.from_numpy(np.asfortranarray(W.kernel_matrix(pts, "matern32", 0.1, 1e-2))).cuda()
+    torch.cuda.synchronize()
+    lib.hodlr_b200_set_option(b"sketch_cap", 32.0)
+    try:
+        def fail_once():
+            with pytest.raises(HodlrError) as e:
+                DeviceTree.build(a.data_ptr(), n, n, 5, 1e-8)
+            assert e.value.code == abi.SVD_FAILURE
+            torch.cuda.synchronize()
+        fail_once()
+        free0 = torch.cuda.mem_get_info()[0]
+        for _ in range(12):
+            fail_once()
+        free1 = torch.cuda.mem_get_info()[0]
+    finally:
+        lib.hodlr_b200_set_option(b"sketch_cap", 1024.0)
+    # each leaked tree would hold about 5 MB (leaves and factors)
+    assert free0 - free1 < 16 * 2 ** 20, (free0, free1)
