@@ -347,10 +347,12 @@ def main():
         # warm-up build on a small leading block initialises the kernels
         DeviceTree.build(a.data_ptr(), 1024, n, 3, tol, stream=sh).free()
         stream.synchronize()
+        torch.cuda.nvtx.range_push("build_plain")
         t0 = time.perf_counter()
         tree = DeviceTree.build(a.data_ptr(), n, n, h, tol, stream=sh)
         stream.synchronize()
         build_s = time.perf_counter() - t0
+        torch.cuda.nvtx.range_pop()
     info = tree.info()
     ranks = tree.ranks()
     plain_stats = build_stats(lib)
@@ -363,10 +365,12 @@ def main():
     try:
         with torch.cuda.stream(stream):
             stream.synchronize()
+            torch.cuda.nvtx.range_push("build_learned")
             t0 = time.perf_counter()
             tree_l = DeviceTree.build(a.data_ptr(), n, n, h, tol, stream=sh)
             stream.synchronize()
             build_s_learned = time.perf_counter() - t0
+            torch.cuda.nvtx.range_pop()
     finally:
         lib.hodlr_b200_set_option(b"learned_ranks", 0.0)
         lib.hodlr_b200_set_option(b"kernel_length", 0.0)
@@ -492,6 +496,26 @@ def main():
     leaves_el = n_leaf * (n // n_leaf) ** 2
     el = {"phase1": sn, "phase2": leaves_el + sn}
     slice_products = 21
+    # int8 operand bytes the mixed kernels must move per phase (6 slices per
+    # value, tiles padded as the kernels lay them out), plus the FP64 W / Y
+    # written: the algorithmic bytes that the measured DRAM traffic is set
+    # against
+    def _cdiv(a_, b_):
+        return -(-a_ // b_)
+    op1 = 6.0 * n * _cdiv(k, 128) * 128
+    op2 = 6.0 * (leaves_el + n * _cdiv(k, 64) * 64) + 8.0 * n * k
+    for b, s_b in enumerate(int(v) for v in ranks):
+        if s_b == 0:
+            continue
+        nb = n >> ((b // 2 + 1).bit_length())
+        ntn = _cdiv(s_b, 64)
+        nw = _cdiv(_cdiv(s_b, ntn), 16) * 16
+        op1 += 6.0 * ntn * nw * nb + 8.0 * s_b * k
+        op2 += 6.0 * nb * _cdiv(s_b, 32) * 32 + 6.0 * _cdiv(s_b, 32) * 32 * _cdiv(k, 64) * 64
+    int8_bytes = {"phase1": op1, "phase2": op2}
+    # DRAM bytes (read + write) per launch / int8 operand bytes, measured by
+    # ncu on the n = 16384 instance (profiles/matmat_mixed_int8_n32768_k256.md)
+    traffic_ratio_i8 = {"phase1": 0.91, "phase2": 0.91}
     peak_i8, peak_src = int8_peak_tops(torch, dev)
     peak64 = fp64_peak_tflops(torch, dev)
     dom = "phase1" if rmx["p1"] >= rmx["p2"] else "phase2"
@@ -542,7 +566,10 @@ def main():
         "gflops": flops_step / (ms_step * 1e-3) / 1e9,
         "roofline": {"bound": "tensor", "kernel": f"ozaki_gemm_kernel ({dom})",
                      "achieved": achieved, "peak": peak_i8, "unit": "TOPS (int8)",
-                     "frac": achieved / peak_i8, "traffic": None,
+                     "frac": achieved / peak_i8,
+                     "traffic": traffic_ratio_i8[dom] * int8_bytes[dom],
+                     "int8_operand_bytes": int8_bytes[dom],
+                     "int8_operand_bytes_by_phase": int8_bytes,
                      "peak_source": peak_src,
                      "phase_ms": {"phase1": rmx["p1"], "phase2": rmx["p2"]}},
         "fp64": {"value": value_fp64, "unit": "GB/s", "ms_per_step": r64["ms"],
