@@ -2,9 +2,10 @@
 // blocked operand layout).
 //
 // Persistent kernel, one CTA of six warps per SM, tiles taken round-robin:
-//   warp 0 (one thread)  producer: per K-block one bulk copy of the A block
-//                        (all S slices of 128 lines) and one of the B block
-//                        into a six-stage ring, completion on full[stage];
+//   warp 0               producer: per K-block the A block (all S slices of
+//                        128 lines) and the B block, each as 1-8 bulk copies
+//                        issued by as many lanes, into a six-stage ring,
+//                        completion on full[stage];
 //   warp 1 (one thread)  MMA issuer: per K-block the S(S+1)/2 slice products
 //                        as 8 MMAs (slice p of A against slices q = 1 .. S+1-p
 //                        of B, which sit next to each other in shared memory,
@@ -12,8 +13,9 @@
 //                        t = p + q - 2 stored side by side in TMEM), commit to
 //                        empty[stage]; after the tile's last K-block a commit
 //                        to tmem_full;
-//   warps 2-5            epilogue: wait tmem_full, read the S int32 groups of
-//                        their 32 TMEM lanes, recombine in FP64, scale by
+//   warps 2-9            epilogue (two warps per quarter of the TMEM lanes,
+//                        alternate 16-column chunks): wait tmem_full, read the
+//                        S int32 groups of their 32 lanes, recombine in FP64, scale by
 //                        2^(e_r + f_j), release the accumulators (tmem_empty),
 //                        store or atomically add the tile.
 // The warp also owns the TMEM allocation (512 columns: S groups of <= 64).
@@ -31,7 +33,8 @@ namespace hb {
 
 namespace {
 
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;                          // two per TMEM lane quarter
+constexpr int kThreads = 32 * (2 + kEpiWarps);
 constexpr int kStages = 6;
 constexpr int kStageBytes = kOzABlock + oz_bblock(kOzMaxNw);   // 36864
 constexpr size_t kSmem = (size_t)kStages * kStageBytes;        // 221184
@@ -49,14 +52,14 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, vo
 
 __global__ void __launch_bounds__(kThreads, 1)
 ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ tiles, int ntiles,
-                  double *cbase, int *status) {
+                  double *cbase, int *status, int split) {
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t empty[kStages];
   __shared__ __align__(8) uint64_t tmem_full, tmem_empty, mma_done;
   __shared__ uint32_t taddr_s;
   __shared__ volatile int bad;
-  __shared__ int cexp_s[4][kOzMaxNw];   // per epilogue warp: column exponents of its tile
+  __shared__ int cexp_s[kEpiWarps][kOzMaxNw];   // per epilogue warp: column exponents of its tile
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 1) {
@@ -69,7 +72,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       umma::mbar_init(&empty[s], 1);
     }
     umma::mbar_init(&tmem_full, 1);
-    umma::mbar_init(&tmem_empty, 4);
+    umma::mbar_init(&tmem_empty, kEpiWarps);
     umma::mbar_init(&mma_done, 1);
     umma::fence_mbar_init();
     bad = 0;
@@ -81,32 +84,47 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
 
   if (warp == 0) {
     // ---------------- producer ----------------
-    if (lane == 0) {
-      long long g = 0;   // K-blocks issued by this CTA
-      for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
-        const OzTile T = tiles[tile];
-        const uint32_t bbytes = (uint32_t)oz_bblock(T.nw);
-        for (int s = T.seg0; s < T.seg0 + T.nseg && !bad; ++s) {
-          const OzSeg G = segs[s];
-          for (int kb = 0; kb < G.nkb; ++kb) {
-            const int st = (int)(g % kStages);
-            const long long use = g / kStages;
-            if (use > 0 && !wait_or_abort(&empty[st], (uint32_t)((use - 1) & 1), &bad)) {
-              bad = 1;
-              break;
-            }
-            uint8_t *dst = sm + st * kStageBytes;
-            umma::mbar_expect_tx(&full[st], (uint32_t)kOzABlock + bbytes);
-            umma::bulk_g2s(dst, G.a + (long long)kb * kOzABlock, kOzABlock, &full[st]);
-            umma::bulk_g2s(dst + kOzABlock, G.b + (long long)kb * bbytes, bbytes, &full[st]);
-            ++g;
+    // lane 0 waits for a free stage and announces its bytes; lanes 0 .. split-1
+    // then each copy 1/split of the A block and of the B block
+    long long g = 0;   // K-blocks issued by this CTA
+    bool stop = false;
+    for (int tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x) {
+      stop = __shfl_sync(0xffffffffu, (int)bad, 0) != 0;
+      if (stop) break;
+      const OzTile T = tiles[tile];
+      const uint32_t bbytes = (uint32_t)oz_bblock(T.nw);
+      const uint32_t ca = (uint32_t)kOzABlock / split, cb = bbytes / split;
+      for (int s = T.seg0; s < T.seg0 + T.nseg && !stop; ++s) {
+        const OzSeg G = segs[s];
+        for (int kb = 0; kb < G.nkb; ++kb) {
+          const int st = (int)(g % kStages);
+          const long long use = g / kStages;
+          int ok = 1;
+          if (lane == 0 && use > 0)
+            ok = wait_or_abort(&empty[st], (uint32_t)((use - 1) & 1), &bad) ? 1 : 0;
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          if (!ok) {
+            if (lane == 0) bad = 1;
+            stop = true;
+            break;
           }
+          uint8_t *dst = sm + st * kStageBytes;
+          if (lane == 0) umma::mbar_expect_tx(&full[st], (uint32_t)kOzABlock + bbytes);
+          __syncwarp();
+          if (lane < split) {
+            umma::bulk_g2s(dst + lane * ca, G.a + (long long)kb * kOzABlock + lane * ca, ca,
+                           &full[st]);
+            umma::bulk_g2s(dst + kOzABlock + lane * cb, G.b + (long long)kb * bbytes + lane * cb,
+                           cb, &full[st]);
+          }
+          ++g;
         }
       }
-      // copies still in flight land before the CTA may exit
+    }
+    // copies still in flight land before the CTA may exit
+    if (lane == 0)
       for (long long q = std::max(0LL, g - kStages); q < g; ++q)
         umma::mbar_wait_bounded(&full[q % kStages], (uint32_t)((q / kStages) & 1), kWaitTries);
-    }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
@@ -160,6 +178,8 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
   } else {
     // ---------------- epilogue ----------------
     const int quarter = warp & 3;   // TMEM lanes 32 quarter .. 32 quarter + 31
+    const int ew = warp - 2;        // epilogue warp 0 .. kEpiWarps - 1
+    const int half = ew >> 2;       // the two warps of a quarter take alternate 16-column chunks
     const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
     const int r = 32 * quarter + lane;
     int lt = 0;
@@ -168,7 +188,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       const OzTile T = tiles[tile];
       // column exponents of this tile, staged while its MMAs run
       __syncwarp();
-      for (int j = lane; j < kOzMaxNw; j += 32) cexp_s[quarter][j] = j < T.cols ? T.cexp[j] : 0;
+      for (int j = lane; j < kOzMaxNw; j += 32) cexp_s[ew][j] = j < T.cols ? T.cexp[j] : 0;
       __syncwarp();
       const bool ready = wait_or_abort(&tmem_full, (uint32_t)(lt & 1), &bad);
       if (!__all_sync(0xffffffffu, ready)) {
@@ -181,7 +201,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       const int er = (row_ok ? T.rexp[r] : 0) - 14;
       double *crow = cbase + T.c_off + r;
       double rowmax = 0.0;
-      for (int c0 = 0; c0 < nw; c0 += 16) {
+      for (int c0 = 16 * half; c0 < nw; c0 += 32) {
         int32_t v[kOzSlices][16];
 #pragma unroll
         for (int t = 0; t < kOzSlices; ++t) umma::tmem_ld16(lane_addr + t * nw + c0, v[t]);
@@ -195,7 +215,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
             double acc = (double)v[kOzSlices - 1][x];
 #pragma unroll
             for (int t = kOzSlices - 2; t >= 0; --t) acc = fma(acc, 0x1p-7, (double)v[t][x]);
-            const int e = er + cexp_s[quarter][j];
+            const int e = er + cexp_s[ew][j];
             const double val = (e >= -1022 && e <= 1023)
                                    ? acc * __longlong_as_double((long long)(e + 1023) << 52)
                                    : ldexp(acc, e);
@@ -437,7 +457,12 @@ void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *
     configured = true;
   }
   const int grid = std::min(ntiles, num_sms());
-  ozaki_gemm_kernel<<<grid, kThreads, kSmem, stream>>>(d_segs, d_tiles, ntiles, cbase, d_status);
+  // bulk copies per operand block (1, 2, 4 or 8 lanes; every chunk stays a
+  // multiple of 16 bytes since B blocks are multiples of 384 bytes)
+  int split = (int)option("ozaki_copy_split", 1.0);
+  split = split >= 8 ? 8 : split >= 4 ? 4 : split >= 2 ? 2 : 1;
+  ozaki_gemm_kernel<<<grid, kThreads, kSmem, stream>>>(d_segs, d_tiles, ntiles, cbase, d_status,
+                                                       split);
   HB_LAUNCHED();
 }
 
