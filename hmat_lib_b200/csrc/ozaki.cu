@@ -270,9 +270,10 @@ __device__ __forceinline__ int find_job(const Job *jobs, int njobs, long long it
 }
 
 constexpr int kMaxChunkK = 2048;   // K values per warp item, K-contiguous lines
-constexpr int kMaxChunkL = 64;     // K values per warp item, line-contiguous (32 lines)
+constexpr int kMaxChunkL = 16;     // K values per warp item, line-contiguous (32 lines)
 constexpr int kTileLines = 32;     // shared-memory transpose tile: lines x K values
-constexpr int kTileK = 128;
+constexpr int kTileK = 64;
+constexpr int kSliceThreads = kTileLines * (kTileK / 16);   // one (line, 16-value chunk) each
 
 __device__ __forceinline__ void max_into(unsigned long long *out, double mx) {
   if (mx > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
@@ -393,10 +394,10 @@ __global__ void slice_lines_kernel(const SliceJob *__restrict__ jobs, int njobs,
   }
 }
 
-// K-contiguous sources (s_k = 1): one block item = 32 lines x 128 K values,
+// K-contiguous sources (s_k = 1): one block item = 32 lines x 64 K values,
 // read with coalesced row loads into shared memory, then sliced 16 K values
-// per thread.
-__global__ void __launch_bounds__(256) slice_kcontig_kernel(const SliceJob *__restrict__ jobs,
+// per thread (small tiles keep a dozen blocks resident per SM).
+__global__ void __launch_bounds__(kSliceThreads) slice_kcontig_kernel(const SliceJob *__restrict__ jobs,
                                                             int njobs, long long items,
                                                             const double *xbase) {
   __shared__ double buf[kTileLines][kTileK + 1];
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(256) slice_kcontig_kernel(const SliceJob *__re
       buf[l][kk] = (line < J.lines && k < J.K) ? src[(long long)line * J.s_line + k] : 0.0;
     }
     __syncthreads();
-    const int l = tid % kTileLines, c = tid / kTileLines;   // 8 chunks of 16
+    const int l = tid % kTileLines, c = tid / kTileLines;   // kTileK / 16 chunks
     const int line = line0 + l, k = k0 + c * 16;
     if (line < J.ntiles * J.R && k < Kw) {
       const bool live = line < J.lines;
@@ -519,8 +520,8 @@ void ozaki_max(const MaxBatch &b, const double *xbase, cudaStream_t stream) {
 void ozaki_slice(const SliceBatch &b, const double *xbase, cudaStream_t stream) {
   if (b.n <= 0 || b.items <= 0) return;
   if (b.kcontig) {
-    const int grid = (int)std::min<long long>(b.items, (long long)num_sms() * 8);
-    slice_kcontig_kernel<<<grid, 256, 0, stream>>>(b.d, b.n, b.items, xbase);
+    const int grid = (int)std::min<long long>(b.items, (long long)num_sms() * 16);
+    slice_kcontig_kernel<<<grid, kSliceThreads, 0, stream>>>(b.d, b.n, b.items, xbase);
   } else {
     slice_lines_kernel<<<grid_for(b.items), 256, 0, stream>>>(b.d, b.n, b.items, xbase);
   }
