@@ -178,18 +178,22 @@ def build_stats(lib):
             "ms_core_svd": st[12], "ms_finish": st[13], "learned_fallbacks": int(st[14])}
 
 
-def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream):
+def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, rank=0, world=1):
     """The uneven batch: `count` HODLRs (n in {1024, 2048, 4096, 8192},
     exponential kernel on sorted 1D points, leaf 128, tol 1e-8), each times a
     dense block of 16-128 columns.  Times one step (all instances) three ways:
     one FP64 product call per tree, the batched FP64 call and the batched
-    mixed-precision call (one launch per phase, graph replay)."""
+    mixed-precision call (one launch per phase, graph replay).  With several
+    ranks the instances are partitioned across them (no collective on the
+    data path); a step's time is the slowest rank's."""
     import numpy as np
 
+    from hmat_lib_b200 import multi
     from hmat_lib_b200 import workloads as W
     from hmat_lib_b200.hodlr import DeviceTree, batched_tuning, matmat_batched
     sh = stream.cuda_stream
-    inst = W.uneven_batch(count, seed=2)
+    everything = W.uneven_batch(count, seed=2)
+    inst = [everything[i] for i in multi.partition(count, rank, world)]
     nmax = max(it["n"] for it in inst)
     trees, xs, ys, ks, ns = [], [], [], [], []
     build_s = 0.0
@@ -214,8 +218,10 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream):
             ns.append(n)
         del a
     torch.cuda.empty_cache()
-    storage = sum(t.info()["storage"] for t in trees)
-    bytes_step = 8.0 * storage + sum(16.0 * n * k for n, k in zip(ns, ks))
+    storage = multi.sum_over_ranks(sum(t.info()["storage"] for t in trees), pg, dev)
+    bytes_step = multi.sum_over_ranks(8.0 * sum(t.info()["storage"] for t in trees) +
+                                      sum(16.0 * n * k for n, k in zip(ns, ks)), pg, dev)
+    build_s = multi.max_over_ranks(build_s, pg, dev)
     xp, yp = [x.data_ptr() for x in xs], [y.data_ptr() for y in ys]
 
     def loop_step():
@@ -236,7 +242,7 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream):
             fn()
         e1.record(stream)
         stream.synchronize()
-        ms = e0.elapsed_time(e1) / nsteps
+        ms = multi.max_over_ranks(e0.elapsed_time(e1) / nsteps, pg, dev)
         return {"ms_per_step": ms, "GB/s": bytes_step / (ms * 1e-3) / 1e9,
                 "gpu_launches_per_step": (lib.hodlr_b200_kernel_launches() - l0) / nsteps}
 
@@ -249,10 +255,13 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream):
     ymx = [torch.zeros_like(y) for y in ys]
     bmx = timed(lambda: batched_step(1, [y.data_ptr() for y in ymx]), nsteps)
     assert lib.hodlr_b200_batched_check() == 0, lib.hodlr_b200_last_error()
-    num = sum(float(torch.linalg.norm(m - f) ** 2) for m, f in zip(ymx, y64b))
-    den = sum(float(torch.linalg.norm(f) ** 2) for f in y64b)
-    numb = sum(float(torch.linalg.norm(b - f) ** 2) for b, f in zip(y64b, y64))
-    out = {"instances": count, "sizes": sorted(set(ns)), "k_range": [min(ks), max(ks)],
+    num = multi.sum_over_ranks(sum(float(torch.linalg.norm(m - f) ** 2)
+                                   for m, f in zip(ymx, y64b)), pg, dev)
+    den = multi.sum_over_ranks(sum(float(torch.linalg.norm(f) ** 2) for f in y64b), pg, dev)
+    numb = multi.sum_over_ranks(sum(float(torch.linalg.norm(b - f) ** 2)
+                                    for b, f in zip(y64b, y64)), pg, dev)
+    out = {"instances": count, "ranks": world, "partition": "instance i on rank i mod ranks",
+           "sizes": sorted(set(ns)), "k_range": [min(ks), max(ks)],
            "kernel": "exp(-|x-y|/l), l ~ U[0.05,0.5], sorted 1D points, seed 2",
            "build_s_total": build_s, "storage_doubles": storage, "bytes_per_step": bytes_step,
            "loop_fp64": loop, "batched_fp64": b64, "batched_mixed": bmx,
@@ -478,7 +487,8 @@ def main():
 
     batch = None
     if args.batch > 0:
-        batch = uneven_batch_bench(args.batch, args.steps, args.warmup, lib, torch, dev, stream)
+        batch = uneven_batch_bench(args.batch, args.steps, args.warmup, lib, torch, dev, stream,
+                                   pg, rank, world)
 
     if rank != 0:
         if pg:
