@@ -358,25 +358,9 @@ int hodlr_b200_build_dev(int height, int n, const int *ms, const double *d_matri
     return INPUT_ERROR;
   }
   try {
-    Geometry g;
-    g.h = height;
     std::vector<int> leaf = ms ? std::vector<int>(ms, ms + (1 << height)) : halves(n, height);
-    g.leaf_m = leaf;
-    g.leaf_off.assign(leaf.size() + 1, 0);
-    for (size_t i = 0; i < leaf.size(); ++i) g.leaf_off[i + 1] = g.leaf_off[i] + leaf[i];
-    HB_REQUIRE(g.leaf_off.back() == n, INPUT_ERROR, "block sizes do not add up to n");
-    g.n = n;
-    g.blocks.resize(g.nblock());
-    for (int d = 0; d < height; ++d)
-      for (int j = 0; j < (1 << d); ++j) {
-        const int span = 1 << (height - d);
-        const long long o = g.leaf_off[j * span], mid = g.leaf_off[j * span + span / 2],
-                        end = g.leaf_off[(j + 1) * span];
-        BlockDesc &tr = g.blocks[block_index(d, j, 1)];
-        BlockDesc &bl = g.blocks[block_index(d, j, 2)];
-        tr = BlockDesc{(int)o, (int)mid, (int)(mid - o), (int)(end - mid), 0, d, 0, 0};
-        bl = BlockDesc{(int)mid, (int)o, (int)(end - mid), (int)(mid - o), 0, d, 0, 0};
-      }
+    Geometry g = geometry_from_leaves(height, leaf);
+    HB_REQUIRE(g.n == n, INPUT_ERROR, "block sizes do not add up to n");
     int status = SUCCESS;
     auto dt = build_from_dense(g, d_matrix, ld, svd_threshold, as_stream(stream), &status);
     *out = new hodlr_b200_tree_s{dt};

@@ -167,6 +167,27 @@ Geometry geometry_of(const TreeHODLR *t) {
   return geometry_of_subtree(t->root, t->height);
 }
 
+Geometry geometry_from_leaves(int h, const std::vector<int> &leaf) {
+  Geometry g;
+  g.h = h;
+  g.leaf_m = leaf;
+  g.leaf_off.assign(leaf.size() + 1, 0);
+  for (size_t i = 0; i < leaf.size(); ++i) g.leaf_off[i + 1] = g.leaf_off[i] + leaf[i];
+  g.n = (int)g.leaf_off.back();
+  g.blocks.resize(g.nblock());
+  for (int d = 0; d < h; ++d)
+    for (int j = 0; j < (1 << d); ++j) {
+      const int span = 1 << (h - d);
+      const long long o = g.leaf_off[j * span], mid = g.leaf_off[j * span + span / 2],
+                      end = g.leaf_off[(j + 1) * span];
+      g.blocks[block_index(d, j, 1)] =
+          BlockDesc{(int)o, (int)mid, (int)(mid - o), (int)(end - mid), 0, d, 0, 0};
+      g.blocks[block_index(d, j, 2)] =
+          BlockDesc{(int)mid, (int)o, (int)(end - mid), (int)(mid - o), 0, d, 0, 0};
+    }
+  return g;
+}
+
 }  // namespace hb
 
 using namespace hb;

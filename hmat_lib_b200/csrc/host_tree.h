@@ -43,6 +43,10 @@ HODLRInternalNode *node_at(HODLRInternalNode *root, int d, int j);
 HODLRLeafNode *diag_leaf(HODLRInternalNode *root, int height, int i);
 
 Geometry geometry_of(const TreeHODLR *t);
+// Geometry of a tree of height h with the given 2^h leaf sizes (ranks 0): the
+// block of child 1 of node (d, j) spans the node's first half of rows and its
+// second half of columns, child 2 the reverse.
+Geometry geometry_from_leaves(int h, const std::vector<int> &leaf);
 Geometry geometry_of_subtree(const HODLRInternalNode *root, int height);
 
 // Drop any device copy registered for this host tree (dtree.cu).

@@ -216,6 +216,21 @@ class DeviceTree:
         if r != abi.SUCCESS:
             raise HodlrError(r, "hodlr_b200_matmat_dev", lib().hodlr_b200_last_error().decode())
 
+    def save(self, path: str):
+        """hodlr_b200_tree_save."""
+        r = lib().hodlr_b200_tree_save(self.h, str(path).encode())
+        if r != abi.SUCCESS:
+            raise HodlrError(r, "hodlr_b200_tree_save", lib().hodlr_b200_last_error().decode())
+
+    @classmethod
+    def load(cls, path: str) -> "DeviceTree":
+        """hodlr_b200_tree_load."""
+        out = C.c_void_p()
+        r = lib().hodlr_b200_tree_load(str(path).encode(), C.byref(out))
+        if r != abi.SUCCESS:
+            raise HodlrError(r, "hodlr_b200_tree_load", lib().hodlr_b200_last_error().decode())
+        return cls(out)
+
     def to_host(self) -> Tree:
         t = Tree(self.info()["height"])
         ierr = C.c_int(0)

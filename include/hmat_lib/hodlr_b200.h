@@ -114,6 +114,16 @@ int hodlr_b200_matvec_noalloc_dev(hodlr_b200_tree t, const double *d_x, double *
 /* Re-upload a host tree whose factor values were edited in place. */
 int hodlr_b200_sync_tree(const struct TreeHODLR *hodlr);
 
+/* Writes a device tree to a file: height, n, leaf sizes, ranks, every leaf and
+ * factor, and a checksum (layout in hmat_lib_b200/csrc/treefile.cpp).  No
+ * counterpart in hmat_lib, which has no serialisation. */
+int hodlr_b200_tree_save(hodlr_b200_tree t, const char *path);
+/* Reads a file written by hodlr_b200_tree_save into a new device tree
+ * (*out, freed with hodlr_b200_tree_free).  A file that is not a tree file,
+ * is truncated or fails its checksum gives INPUT_ERROR and leaves *out
+ * untouched. */
+int hodlr_b200_tree_load(const char *path, hodlr_b200_tree *out);
+
 /* Y_i = op(H_i) X_i for i < count, every tree of the batch (any sizes, ranks
  * and heights) in one launch per phase.  Device pointers, column-major;
  * k[i] columns of X_i / Y_i (rows for op L), leading dimensions ldx[i],
