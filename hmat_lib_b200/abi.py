@@ -152,6 +152,9 @@ B200_API = {
     "hodlr_b200_rank_model_gradient": (C.c_int, [FP, FP, FP, C.c_int, FP, FP]),
     "hodlr_b200_rank_model_adam": (C.c_int, [FP, FP, FP, FP, C.c_int, C.c_double]),
     "hodlr_b200_build_features": (C.c_int, [FP, C.c_int]),
+    "hodlr_b200_build_kernel_dev": (
+        C.c_int, [C.c_int, C.c_int, IP, VP, C.c_int, C.c_int, C.c_double, C.c_double,
+                  C.c_double, C.c_int, VP, C.POINTER(VP), IP]),
     "hodlr_b200_tree_save": (C.c_int, [VP, C.c_char_p]),
     "hodlr_b200_tree_load": (C.c_int, [C.c_char_p, C.POINTER(VP)]),
 }

@@ -388,6 +388,38 @@ int hodlr_b200_tree_to_host(hodlr_b200_tree t, TreeHODLR *hodlr, int *ierr) {
   }
 }
 
+int hodlr_b200_build_kernel_dev(int height, int n, const int *ms, const double *d_points,
+                                int dim, int kind, double length, double diag,
+                                double svd_threshold, int flags, void *stream,
+                                hodlr_b200_tree *out, int *ierr) {
+  (void)flags;
+  if (!d_points || !out || height < 1 || n < 0 || dim < 1 || kind < 0 || kind > 2 ||
+      !(length > 0.0)) {
+    if (ierr) *ierr = INPUT_ERROR;
+    return INPUT_ERROR;
+  }
+  try {
+    std::vector<int> leaf = ms ? std::vector<int>(ms, ms + (1 << height)) : halves(n, height);
+    Geometry g = geometry_from_leaves(height, leaf);
+    HB_REQUIRE(g.n == n, INPUT_ERROR, "block sizes do not add up to n");
+    KernelSpec K;
+    K.pts = d_points;
+    K.n = n;
+    K.dim = dim;
+    K.kind = kind;
+    K.length = length;
+    K.diag = diag;
+    int status = SUCCESS;
+    auto dt = build_from_dense(g, nullptr, n, svd_threshold, as_stream(stream), &status,
+                               nullptr, &K);
+    *out = new hodlr_b200_tree_s{dt};
+    if (ierr) *ierr = status;
+    return status;
+  } catch (const Error &e) {
+    return fail(ierr, e);
+  }
+}
+
 hodlr_b200_tree hodlr_b200_tree_from_host(const TreeHODLR *hodlr, int *ierr) {
   try {
     auto dt = device_tree_for(hodlr, lib_stream());

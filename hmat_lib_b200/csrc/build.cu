@@ -26,6 +26,7 @@
 #include "jacobi.h"
 #include "rank_mlp.h"
 #include "tsqr.h"
+#include "workload.h"
 
 namespace hb {
 
@@ -67,7 +68,8 @@ constexpr int kFeatCols = 16;   // width of the feature sketch
 // of R (= those of Y) by the batched Jacobi SVD, then log block size, depth,
 // ln(kernel length) and five log ratios of the sketch's singular values.
 std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlock> &sk,
-                                  const double *d_A, long long lda, unsigned long long seed,
+                                  const double *d_A, long long lda, int aslot,
+                                  const KernelSpec &gen, unsigned long long seed,
                                   cudaStream_t stream) {
   const int nsk = (int)sk.size();
   std::vector<float> f((size_t)nsk * kRankIn, 0.f);
@@ -103,11 +105,12 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
   GemmBases bases{};
   bases.p[0] = const_cast<double *>(d_A);
   for (int i = 1; i < kGemmBases; ++i) bases.p[i] = w;
+  bases.gen = gen;
   GemmBatch gb;
   for (int i = 0; i < nsk; ++i) {
     const SketchBlock &S = sk[i];
     int pr = gb.add(1, y[i], S.m, S.m, F);
-    gb.seg(pr, 0, S.a_off, lda, 0, 1, om[i], S.n, 0, S.n);
+    gb.seg(pr, aslot, S.a_off, lda, 0, 1, om[i], S.n, 0, S.n);
   }
   gemm_f64_run(gb, bases, TileShape::M128N64, stream);
   std::vector<TsqrProb> tp;
@@ -175,7 +178,8 @@ const std::vector<float> &last_build_features() { return g_last_features; }
 
 std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double *d_A,
                                              long long lda, double tol, cudaStream_t stream,
-                                             int *svd_status, BuildStats *stats) {
+                                             int *svd_status, BuildStats *stats,
+                                             const KernelSpec *gen) {
   auto t0 = std::chrono::steady_clock::now();
   Geometry g = g_in;
   const int nb = g.nblock();
@@ -186,6 +190,9 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   const int w_next = std::max(kPanel, (int)option("sketch_step", 64) / kPanel * kPanel);
   const double eta = option("sketch_eta", 0.01);
   const unsigned long long seed = (unsigned long long)option("sketch_seed", 20240607);
+  // operand of the block reads: the dense input, or the generated kernel matrix
+  const KernelSpec gspec = gen ? *gen : KernelSpec();
+  const int aslot = gen ? (int)kGenSlot : (int)kA;
 
   // ---- partition the blocks --------------------------------------------------
   std::vector<int> exact, sketched;
@@ -225,7 +232,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     S.m = B.m;
     S.n = B.n;
     S.cap = std::min(std::min(B.m, B.n), std::max(cap_max, kPanel));
-    S.a_off = B.r0 + (long long)B.c0 * lda;
+    S.a_off = gen ? gen_offset(B.r0, B.c0) : B.r0 + (long long)B.c0 * lda;
     sk.push_back(S);
   }
   // ---- learned sizing of the first sketch ---------------------------------------------
@@ -237,7 +244,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   for (SketchBlock &S : sk) S.first_w = std::min(w_first, S.cap);
   const auto tf0 = std::chrono::steady_clock::now();
   if (record && !sk.empty()) {
-    feats = block_features(g, sk, d_A, lda, seed, stream);
+    feats = block_features(g, sk, d_A, lda, aslot, gspec, seed, stream);
     if (have_model) {
       const int nsk = (int)sk.size();
       float *dbuf = nullptr;
@@ -289,6 +296,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   double *work = dev_alloc(scratch, stream);
   GemmBases bases{};
   bases.p[kA] = const_cast<double *>(d_A);
+  bases.gen = gspec;
   bases.p[kWork] = work;
   for (int i = 2; i < kGemmBases; ++i) bases.p[i] = work;
   if (!sk.empty()) HB_CUDA(cudaMemsetAsync(work, 0, scratch * sizeof(double), stream));
@@ -318,7 +326,12 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     const BlockDesc &B = g.blocks[exact[p]];
     const int R = std::max(B.m, B.n), C = std::min(B.m, B.n);
     JacobiProb jp{};
-    jp.A = d_A + B.r0 + (long long)B.c0 * lda;
+    if (gen) {
+      jp.gen_r0 = B.r0;
+      jp.gen_c0 = B.c0;
+    } else {
+      jp.A = d_A + B.r0 + (long long)B.c0 * lda;
+    }
     jp.lda = lda;
     jp.transA = 0;
     jp.m = B.m;
@@ -337,7 +350,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   JacobiProb *d_eprobs = nullptr;
   if (!eprobs.empty()) {
     d_eprobs = upload_vec(eprobs, stream);
-    jacobi_svd_batched(d_eprobs, (int)eprobs.size(), prm, d_status, max_c, stream);
+    jacobi_svd_batched(d_eprobs, (int)eprobs.size(), prm, d_status, max_c, stream, gspec);
   }
 
   HB_CUDA(cudaEventRecord(ev[1], stream));
@@ -377,7 +390,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
       for (int i : act) {
         const SketchBlock &S = sk[i];
         int pr = g1.add(kWork, S.q + (long long)S.ell * S.m, S.m, S.m, wb[i]);
-        g1.seg(pr, kA, S.a_off, lda, 0, kWork, S.om, S.n, 0, S.n);
+        g1.seg(pr, aslot, S.a_off, lda, 0, kWork, S.om, S.n, 0, S.n);
       }
       gemm_f64_run(g1, bases, TileShape::M128N64, stream);
       // ||A om_c||^2: the scale against which a projected column counts as noise
@@ -494,7 +507,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
       for (int i : act) {
         const SketchBlock &S = sk[i];
         int pr = g5.add(kWork, S.bt + (long long)S.ell * S.n, S.n, S.n, wb[i]);
-        g5.seg(pr, kA, S.a_off, lda, 1, kWork, S.q + (long long)S.ell * S.m, S.m, 0, S.m);
+        g5.seg(pr, aslot, S.a_off, lda, 1, kWork, S.q + (long long)S.ell * S.m, S.m, 0, S.m);
       }
       gemm_f64_run(g5, bases, TileShape::M128N64, stream);
       std::vector<CopyDesc> cp;
@@ -633,12 +646,17 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   // ---- arena: leaves from the input, factors from the scratch ------------------------
   std::shared_ptr<DeviceTree> dt = dtree_create(g, stream);
   std::vector<CopyDesc> copies;
+  std::vector<GenBlock> gen_leaves;
   for (int i = 0; i < g.nleaf(); ++i) {
     const LeafDesc &L = dt->leaves[i];
     if (L.m == 0) continue;
-    copies.push_back(
-        CopyDesc{d_A + L.r0 + (long long)L.r0 * lda, lda, dt->arena + L.off, L.m, L.m, L.m});
+    if (gen)
+      gen_leaves.push_back(GenBlock{L.r0, L.r0, L.m, L.m, dt->arena + L.off, L.m});
+    else
+      copies.push_back(
+          CopyDesc{d_A + L.r0 + (long long)L.r0 * lda, lda, dt->arena + L.off, L.m, L.m, L.m});
   }
+  kernel_blocks(gspec, gen_leaves, stream);
   for (size_t p = 0; p < exact.size(); ++p) {
     const BlockDesc &B = dt->g.blocks[exact[p]];
     if (B.s == 0) continue;

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "dtree.h"
+#include "kernelspec.cuh"
 
 namespace hb {
 
@@ -40,8 +41,12 @@ const std::vector<float> &last_build_features();
 // Compresses every off-diagonal block of the n x n matrix d_A (ld lda, device)
 // following the block sizes of `g` (ranks ignored) with hmat_lib's relative
 // truncation rule at `tol`.  `svd_status` receives SUCCESS or SVD_FAILURE.
+// With `gen` set, the matrix is the kernel matrix it defines and is never
+// formed: every entry the build needs is computed where it is used (d_A and
+// lda are then ignored).
 std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g, const double *d_A, long long lda,
                                              double tol, cudaStream_t stream, int *svd_status,
-                                             BuildStats *stats = nullptr);
+                                             BuildStats *stats = nullptr,
+                                             const KernelSpec *gen = nullptr);
 
 }  // namespace hb

@@ -86,10 +86,25 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
     }
   };
 
+  // One operand element into shared memory: copied from global memory, or
+  // computed when the segment's operand is a generated kernel matrix (stored
+  // element (row, col) of the block at gen_offset(row0, col0)).
+  auto stage = [&](double *dst, bool gen, const double *base, long long off, long long row,
+                   long long col, long long ld, bool p) {
+    if (gen) {
+      *dst = p ? kernel_entry(bases.gen, (int)(off >> 32) + (int)row,
+                              (int)(off & 0xffffffffLL) + (int)col)
+               : 0.0;
+    } else {
+      cp_async8(dst, p ? base + off + row + col * ld : base, p);
+    }
+  };
+
   auto load = [&](int buf, const KIter &it) {
     const GemmSeg S = segs[it.si];
-    const double *A = bases.p[S.abase] + S.a_off;
-    const double *B = bases.p[S.bbase] + S.b_off;
+    const bool ga = S.abase == kGenSlot, gb = S.bbase == kGenSlot;
+    const double *A = ga ? nullptr : bases.p[S.abase];
+    const double *B = gb ? nullptr : bases.p[S.bbase];
     double *as = As + buf * kBK * LDA;
     double *bs = Bs + buf * kBK * LDB;
     const int kk = it.kk, kend = it.le;
@@ -101,8 +116,7 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
       for (int i = 0; i < BM * kBK / kThreads; ++i) {
         const int k = tid / BM + KS * i;
         const bool p = mok && (kk + k) < kend;
-        const double *src = p ? A + (tile.m0 + m) + (long long)(kk + k) * S.lda : A;
-        cp_async8(as + k * LDA + m, src, p);
+        stage(as + k * LDA + m, ga, A, S.a_off, tile.m0 + m, kk + k, S.lda, p);
       }
     } else {
       const int k = tid & 15;
@@ -111,8 +125,7 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
       for (int i = 0; i < BM / 16; ++i) {
         const int m = (tid >> 4) + 16 * i;
         const bool p = kok && (tile.m0 + m) < P.M;
-        const double *src = p ? A + (kk + k) + (long long)(tile.m0 + m) * S.lda : A;
-        cp_async8(as + k * LDA + m, src, p);
+        stage(as + k * LDA + m, ga, A, S.a_off, kk + k, tile.m0 + m, S.lda, p);
       }
     }
     if (S.tb == 0) {
@@ -122,8 +135,7 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
       for (int i = 0; i < BN / 16; ++i) {
         const int n = (tid >> 4) + 16 * i;
         const bool p = kok && (tile.n0 + n) < P.N;
-        const double *src = p ? B + (kk + k) + (long long)(tile.n0 + n) * S.ldb : B;
-        cp_async8(bs + k * LDB + n, src, p);
+        stage(bs + k * LDB + n, gb, B, S.b_off, kk + k, tile.n0 + n, S.ldb, p);
       }
     } else {
       constexpr int KS = kThreads / BN;
@@ -133,8 +145,7 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
       for (int i = 0; i < BN * kBK / kThreads; ++i) {
         const int k = tid / BN + KS * i;
         const bool p = nok && (kk + k) < kend;
-        const double *src = p ? B + (tile.n0 + n) + (long long)(kk + k) * S.ldb : B;
-        cp_async8(bs + k * LDB + n, src, p);
+        stage(bs + k * LDB + n, gb, B, S.b_off, tile.n0 + n, kk + k, S.ldb, p);
       }
     }
   };

@@ -16,13 +16,18 @@
 #include <vector>
 
 #include "common.h"
+#include "kernelspec.cuh"
 
 namespace hb {
 
 constexpr int kGemmBases = 6;
 
+// Base addresses of the launch; `gen` defines the operands of base slot
+// kGenSlot (kernel-matrix entries computed in the loaders, offset =
+// gen_offset(row0, col0) of the block, leading dimension unused).
 struct GemmBases {
   double *p[kGemmBases];
+  KernelSpec gen;
 };
 
 struct GemmSeg {

@@ -64,7 +64,7 @@ __device__ __forceinline__ void team_sync() {
 // CTAs' shared memory.  Every pair's arithmetic is the same in both modes.
 template <bool kTeam>
 __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *status,
-                             int crank, int team) {
+                             int crank, int team, const KernelSpec &gen) {
   const int m = P.m, n = P.n;
   const bool tall = m >= n;
   const int R = tall ? m : n, C = tall ? n : m;
@@ -81,7 +81,13 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
     const int r = (int)(e % R), c = (int)(e / R);
     // logical element (i, j) of the m x n input
     const int i = tall ? r : c, j = tall ? c : r;
-    gst<kTeam>(G + e, P.transA ? P.A[j + (long long)i * P.lda] : P.A[i + (long long)j * P.lda]);
+    double a;
+    if (P.gen_r0 >= 0)
+      a = P.transA ? kernel_entry(gen, P.gen_r0 + j, P.gen_c0 + i)
+                   : kernel_entry(gen, P.gen_r0 + i, P.gen_c0 + j);
+    else
+      a = P.transA ? P.A[j + (long long)i * P.lda] : P.A[i + (long long)j * P.lda];
+    gst<kTeam>(G + e, a);
   }
   for (long long e = gtid; e < (long long)C * C; e += gthreads)
     gst<kTeam>(W + e, ((e % C) == (e / C)) ? 1.0 : 0.0);
@@ -237,14 +243,15 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
 
 // One CTA per problem.
 __global__ void __launch_bounds__(kJThreads)
-jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *status) {
+jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *status,
+                  KernelSpec gen) {
   const JacobiProb P = probs[blockIdx.x];
   const int C = P.m < P.n ? P.m : P.n;
   if (C == 0) {
     if (threadIdx.x == 0 && P.rank) *P.rank = 0;
     return;
   }
-  jacobi_solve<false>(P, prm, status, 0, 1);
+  jacobi_solve<false>(P, prm, status, 0, 1, gen);
 }
 
 // A cluster of kJCluster CTAs per problem; problems with at least
@@ -252,7 +259,7 @@ jacobi_svd_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *s
 // first CTA alone (the rest return at once, before any cluster barrier).
 __global__ void __cluster_dims__(kJCluster, 1, 1) __launch_bounds__(kJThreads)
 jacobi_svd_cluster_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm, int *status,
-                          int team_min_c) {
+                          int team_min_c, KernelSpec gen) {
   const int crank = (int)cg::this_cluster().block_rank();
   const JacobiProb P = probs[blockIdx.x / kJCluster];
   const int C = P.m < P.n ? P.m : P.n;
@@ -261,10 +268,10 @@ jacobi_svd_cluster_kernel(const JacobiProb *__restrict__ probs, JacobiParams prm
     return;
   }
   if (C >= team_min_c) {
-    jacobi_solve<true>(P, prm, status, crank, kJCluster);
+    jacobi_solve<true>(P, prm, status, crank, kJCluster, gen);
   } else {
     if (crank != 0) return;
-    jacobi_solve<false>(P, prm, status, 0, 1);
+    jacobi_solve<false>(P, prm, status, 0, 1, gen);
   }
 }
 
@@ -291,7 +298,7 @@ __global__ void add2d_kernel(const CopyDesc *__restrict__ descs, double alpha) {
 }  // namespace
 
 void jacobi_svd_batched(const JacobiProb *d_probs, int nprobs, const JacobiParams &prm,
-                        int *d_status, int max_c, cudaStream_t stream) {
+                        int *d_status, int max_c, cudaStream_t stream, const KernelSpec &gen) {
   if (nprobs <= 0) return;
   const size_t smem = (size_t)std::max(max_c, 1) * (sizeof(double) + sizeof(int));
   HB_REQUIRE(smem <= 200 * 1024, INPUT_ERROR, "Jacobi SVD problem too wide for one CTA");
@@ -302,13 +309,13 @@ void jacobi_svd_batched(const JacobiProb *d_probs, int nprobs, const JacobiParam
     if (smem > 48 * 1024)
       HB_CUDA(cudaFuncSetAttribute(jacobi_svd_cluster_kernel,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    jacobi_svd_cluster_kernel<<<nprobs * kJCluster, kJThreads, smem, stream>>>(d_probs, prm,
-                                                                            d_status, team_min_c);
+    jacobi_svd_cluster_kernel<<<nprobs * kJCluster, kJThreads, smem, stream>>>(
+        d_probs, prm, d_status, team_min_c, gen);
   } else {
     if (smem > 48 * 1024)
       HB_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
-    jacobi_svd_kernel<<<nprobs, kJThreads, smem, stream>>>(d_probs, prm, d_status);
+    jacobi_svd_kernel<<<nprobs, kJThreads, smem, stream>>>(d_probs, prm, d_status, gen);
   }
   HB_LAUNCHED();
 }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.h"
+#include "kernelspec.cuh"
 
 namespace hb {
 
@@ -23,6 +24,8 @@ struct JacobiProb {
   double *sigma;    // out: C singular values, descending
   int *rank;        // out: truncation rank (>= 1 unless the block is empty)
   int *sweeps;      // out (optional): sweeps used; max_sweeps + 1 if not converged
+  int gen_r0 = -1;  // >= 0: A is the block of the launch's kernel matrix with origin
+  int gen_c0 = 0;   //   (gen_r0, gen_c0) (element (i, j) computed, A / lda unused)
 };
 
 enum class Truncation : int {
@@ -50,7 +53,8 @@ inline long long jacobi_workspace(int m, int n) {
 // status: device int, set to SVD_FAILURE by any problem that did not
 // converge within max_sweeps (left untouched otherwise).
 void jacobi_svd_batched(const JacobiProb *d_probs, int nprobs, const JacobiParams &prm,
-                        int *d_status, int max_c, cudaStream_t stream);
+                        int *d_status, int max_c, cudaStream_t stream,
+                        const KernelSpec &gen = KernelSpec());
 
 struct CopyDesc {
   const double *src;

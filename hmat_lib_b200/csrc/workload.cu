@@ -2,34 +2,30 @@
 // A_ij = k(|p_i - p_j|) + diag * delta_ij, column-major.  Lets a caller build
 // a HODLR of a kernel matrix without forming it on the host.
 #include "../../include/hmat_lib/hodlr_b200.h"
-#include "common.h"
+#include "kernelspec.cuh"
+#include "workload.h"
 
 namespace hb {
 namespace {
 
-__global__ void kernel_matrix_kernel(const double *__restrict__ pts, int n, int dim, int kind,
-                                     double length, double diag, double *__restrict__ out,
-                                     long long ld, int j0) {
+__global__ void kernel_matrix_kernel(KernelSpec K, double *__restrict__ out, long long ld,
+                                     int j0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;   // row: consecutive threads
   const int j = j0 + blockIdx.y;
-  if (i >= n) return;
-  double r2 = 0.0;
-  for (int a = 0; a < dim; ++a) {
-    const double d = pts[i + (long long)a * n] - pts[j + (long long)a * n];
-    r2 = fma(d, d, r2);
+  if (i >= K.n) return;
+  out[i + (long long)j * ld] = kernel_entry(K, i, j);
+}
+
+// rows x cols sub-blocks of the kernel matrix (origins r0, c0) into dense
+// column-major destinations
+__global__ void kernel_blocks_kernel(KernelSpec K, const GenBlock *__restrict__ blocks) {
+  const GenBlock B = blocks[blockIdx.y];
+  const long long total = (long long)B.rows * B.cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e % B.rows), c = (int)(e / B.rows);
+    B.dst[r + (long long)c * B.ld] = kernel_entry(K, B.r0 + r, B.c0 + c);
   }
-  const double r = sqrt(r2);
-  double v;
-  if (kind == 0) {
-    v = exp(-r2 / (2.0 * length * length));           // Gaussian
-  } else if (kind == 1) {
-    const double t = 1.7320508075688772 * r / length;  // Matern-3/2
-    v = (1.0 + t) * exp(-t);
-  } else {
-    v = exp(-r / length);                              // exponential
-  }
-  if (i == j) v += diag;
-  out[i + (long long)j * ld] = v;
 }
 
 }  // namespace
@@ -43,10 +39,32 @@ extern "C" int hodlr_b200_kernel_matrix_dev(const double *d_points, int n, int d
   if (n == 0) return SUCCESS;
   for (int j0 = 0; j0 < n; j0 += 65535) {
     dim3 grid((n + 255) / 256, std::min(65535, n - j0));
-    hb::kernel_matrix_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(
-        d_points, n, dim, kind, length, diag, d_out, ld, j0);
+    hb::KernelSpec K;
+    K.pts = d_points;
+    K.n = n;
+    K.dim = dim;
+    K.kind = kind;
+    K.length = length;
+    K.diag = diag;
+    hb::kernel_matrix_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(K, d_out, ld, j0);
     hb::count_launch();
     if (cudaGetLastError() != cudaSuccess) return ALLOCATION_FAILURE;
   }
   return SUCCESS;
 }
+
+namespace hb {
+void kernel_blocks(const KernelSpec &K, const std::vector<GenBlock> &blocks, cudaStream_t stream) {
+  if (blocks.empty()) return;
+  GenBlock *d = nullptr;
+  HB_CUDA(cudaMallocAsync((void **)&d, sizeof(GenBlock) * blocks.size(), stream));
+  HB_CUDA(cudaMemcpyAsync(d, blocks.data(), sizeof(GenBlock) * blocks.size(),
+                          cudaMemcpyHostToDevice, stream));
+  for (size_t off = 0; off < blocks.size(); off += 65535) {
+    dim3 grid(64, (unsigned)std::min<size_t>(65535, blocks.size() - off));
+    kernel_blocks_kernel<<<grid, 256, 0, stream>>>(K, d + off);
+    HB_LAUNCHED();
+  }
+  cudaFreeAsync(d, stream);
+}
+}  // namespace hb

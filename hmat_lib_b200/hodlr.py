@@ -189,6 +189,28 @@ class DeviceTree:
         return cls(out)
 
     @classmethod
+    def build_kernel(cls, d_points_ptr: int, n: int, dim: int, kind: int, length: float,
+                     diag: float, height: int, tol: float, stream: int = 0,
+                     ms=None) -> "DeviceTree":
+        """hodlr_b200_build_kernel_dev: the tree of a kernel matrix that is
+        never formed (points column-major n x dim on the device)."""
+        out = C.c_void_p()
+        ierr = C.c_int(0)
+        msp = None
+        if ms is not None:
+            arr = (C.c_int * len(ms))(*ms)
+            msp = C.cast(arr, abi.IP)
+        lib().hodlr_b200_build_kernel_dev(height, n, msp, C.c_void_p(d_points_ptr), dim, kind,
+                                          length, diag, tol, 0, C.c_void_p(stream),
+                                          C.byref(out), C.byref(ierr))
+        if ierr.value != abi.SUCCESS and out.value:
+            msg = lib().hodlr_b200_last_error().decode()
+            lib().hodlr_b200_tree_free(out)
+            raise HodlrError(ierr.value, "hodlr_b200_build_kernel_dev", msg)
+        _check(ierr, "hodlr_b200_build_kernel_dev")
+        return cls(out)
+
+    @classmethod
     def of_host(cls, tree: Tree) -> "DeviceTree":
         ierr = C.c_int(0)
         h = lib().hodlr_b200_tree_from_host(tree.tp, C.byref(ierr))

@@ -77,6 +77,19 @@ int hodlr_b200_check(hodlr_b200_tree t, void *stream);
 /* H1 * H2 with recompression at svd_threshold, result stays on the device. */
 int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshold,
                        hodlr_b200_tree *out, int *ierr);
+/* Build of the kernel matrix A_ij = k(|p_i - p_j|) + diag delta_ij (points
+ * and kinds as for hodlr_b200_kernel_matrix_dev below) without forming it:
+ * every entry the construction needs is computed on the device where it is
+ * used, so memory holds only the points, the tree and the sketches (a dense
+ * n = 65536 input would take 34 GB).  The tree equals the one
+ * hodlr_b200_build_dev makes from the generated dense matrix.  No
+ * counterpart in hmat_lib, whose constructor takes the dense matrix
+ * (dense_to_tree_hodlr, src/constructors.c:629).  Ownership and errors as for
+ * hodlr_b200_build_dev. */
+int hodlr_b200_build_kernel_dev(int height, int n, const int *ms, const double *d_points,
+                                int dim, int kind, double length, double diag,
+                                double svd_threshold, int flags, void *stream,
+                                hodlr_b200_tree *out, int *ierr);
 /* Kernel matrix in device memory: out_ij = k(|p_i - p_j|) + diag delta_ij,
  * points column-major n x dim (coordinate a of point i at d_points[i + a n]);
  * kind 0: exp(-r^2 / (2 l^2)), 1: Matern-3/2 (1 + sqrt(3) r / l) exp(-sqrt(3) r / l),
