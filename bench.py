@@ -366,6 +366,20 @@ def main():
     ranks = tree.ranks()
     plain_stats = build_stats(lib)
 
+    # ---- matrix-free build: the same tree from the points, no n x n matrix ------------
+    with torch.cuda.stream(stream):
+        stream.synchronize()
+        torch.cuda.nvtx.range_push("build_matrix_free")
+        t0 = time.perf_counter()
+        tree_mf = DeviceTree.build_kernel(d_pts.data_ptr(), n, pts.shape[1], kind, w["length"],
+                                          w["diag"], h, tol, stream=sh)
+        stream.synchronize()
+        build_s_mf = time.perf_counter() - t0
+        torch.cuda.nvtx.range_pop()
+    mf_stats = build_stats(lib)
+    mf_rank_diff = int(np.max(np.abs(tree_mf.ranks() - ranks)))
+    tree_mf.free()
+
     # ---- learned build: sketches sized in one shot by the shipped rank model ------
     from hmat_lib_b200 import rank_model as RM
     RM.load_default()
@@ -455,6 +469,36 @@ def main():
     value = bytes_step * world / (rmx["ms"] * 1e-3) / 1e9
     value_fp64 = bytes_step * world / (r64["ms"] * 1e-3) / 1e9
     ms_step = rmx["ms"]
+
+    # ---- direct solve: factorise once, then X = A^-1 B through the factor ---------------
+    tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)     # B = A x (FP64)
+    stream.synchronize()
+    torch.cuda.nvtx.range_push("factorize")
+    t0 = time.perf_counter()
+    fac = tree.factorize(stream=sh)
+    factor_s = time.perf_counter() - t0
+    torch.cuda.nvtx.range_pop()
+    xs = torch.zeros_like(x)
+    fac.solve(y.data_ptr(), k, n, xs.data_ptr(), n, stream=sh)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    solve_reps = 5
+    torch.cuda.nvtx.range_push("solve")
+    e0.record(stream)
+    for _ in range(solve_reps):
+        fac.solve(y.data_ptr(), k, n, xs.data_ptr(), n, stream=sh)
+    e1.record(stream)
+    stream.synchronize()
+    torch.cuda.nvtx.range_pop()
+    solve_ms = e0.elapsed_time(e1) / solve_reps
+    r_solve = torch.zeros_like(y)
+    tree.matmat(xs.data_ptr(), k, n, r_solve.data_ptr(), n, stream=sh)
+    stream.synchronize()
+    solve_info = {"factorize_s": factor_s, "ms_per_solve": solve_ms, "rhs": k,
+                  "residual": (torch.linalg.norm(r_solve - y) / torch.linalg.norm(y)).item(),
+                  "rel_err_vs_x": (torch.linalg.norm(xs - x) / torch.linalg.norm(x)).item()}
+    fac.free()
+    del xs, r_solve
 
     # ---- e2e through the C-ABI with host buffers ------------------------------------
     host_tree = tree.to_host()
@@ -565,11 +609,15 @@ def main():
                   "learned": dict(seconds=build_s_learned, rel_err_vs_dense=rel_err_learned,
                                   max_rank_diff_vs_plain=int(np.max(np.abs(ranks_l - ranks))),
                                   **learned_stats),
+                  "matrix_free": dict(seconds=build_s_mf, max_rank_diff_vs_plain=mf_rank_diff,
+                                      input="points only (hodlr_b200_build_kernel_dev)",
+                                      **mf_stats),
                   "speedup_learned_vs_plain": build_s / build_s_learned,
                   "model": "hmat_lib_b200/rank_model.f32 (MLP 8-64-64-1, trained by the "
                            "library's GPU kernels)"},
         "rel_err_vs_dense": rel_err,
         "rel_err_mixed_vs_fp64": rel_err_mixed_vs_fp64,
+        "solve": solve_info,
         "tree": {"max_rank": info["max_rank"], "storage_doubles": storage,
                  "ranks_by_depth": [int(max(ranks[2 * ((1 << d) - 1):2 * ((1 << (d + 1)) - 1)]))
                                     for d in range(h)]},

@@ -155,6 +155,9 @@ B200_API = {
     "hodlr_b200_build_kernel_dev": (
         C.c_int, [C.c_int, C.c_int, IP, VP, C.c_int, C.c_int, C.c_double, C.c_double,
                   C.c_double, C.c_int, VP, C.POINTER(VP), IP]),
+    "hodlr_b200_factorize_dev": (C.c_int, [VP, VP, C.POINTER(VP), IP]),
+    "hodlr_b200_solve_dev": (C.c_int, [VP, VP, C.c_int, C.c_int, VP, C.c_int, VP]),
+    "hodlr_b200_factor_free": (None, [VP]),
     "hodlr_b200_tree_save": (C.c_int, [VP, C.c_char_p]),
     "hodlr_b200_tree_load": (C.c_int, [C.c_char_p, C.POINTER(VP)]),
 }

@@ -17,6 +17,7 @@
 #include "hxh.h"
 #include "products.h"
 #include "rank_mlp.h"
+#include "solve.h"
 
 using namespace hb;
 
@@ -419,6 +420,51 @@ int hodlr_b200_build_kernel_dev(int height, int n, const int *ms, const double *
     return fail(ierr, e);
   }
 }
+
+}  // extern "C"
+
+struct hodlr_b200_factor_s {
+  std::unique_ptr<HodlrFactor> f;
+};
+
+extern "C" {
+
+int hodlr_b200_factorize_dev(hodlr_b200_tree t, void *stream, hodlr_b200_factor *out, int *ierr) {
+  if (!t || !out) {
+    if (ierr) *ierr = INPUT_ERROR;
+    return INPUT_ERROR;
+  }
+  try {
+    int status = SUCCESS;
+    auto f = hodlr_factorize(t->p, as_stream(stream), &status);
+    if (status != SUCCESS) {
+      set_last_error("factorisation: a leaf or capacitance matrix is singular to working precision");
+      if (ierr) *ierr = status;
+      return status;
+    }
+    *out = new hodlr_b200_factor_s{std::move(f)};
+    if (ierr) *ierr = SUCCESS;
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(ierr, e);
+  }
+}
+
+int hodlr_b200_solve_dev(hodlr_b200_factor f, const double *d_b, int k, int ldb, double *d_x,
+                         int ldx, void *stream) {
+  if (!f || !d_b || !d_x || d_b == d_x || k < 0) return INPUT_ERROR;
+  try {
+    const int n = f->f->tree->g.n;
+    HB_REQUIRE(ldb >= std::max(1, n) && ldx >= std::max(1, n), INPUT_ERROR,
+               "leading dimension below n");
+    hodlr_solve(*f->f, d_b, k, ldb, d_x, ldx, as_stream(stream));
+    return SUCCESS;
+  } catch (const Error &e) {
+    return fail(nullptr, e);
+  }
+}
+
+void hodlr_b200_factor_free(hodlr_b200_factor f) { delete f; }
 
 hodlr_b200_tree hodlr_b200_tree_from_host(const TreeHODLR *hodlr, int *ierr) {
   try {

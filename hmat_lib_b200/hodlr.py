@@ -253,6 +253,14 @@ class DeviceTree:
             raise HodlrError(r, "hodlr_b200_tree_load", lib().hodlr_b200_last_error().decode())
         return cls(out)
 
+    def factorize(self, stream: int = 0) -> "Factor":
+        """hodlr_b200_factorize_dev."""
+        out = C.c_void_p()
+        ierr = C.c_int(0)
+        lib().hodlr_b200_factorize_dev(self.h, C.c_void_p(stream), C.byref(out), C.byref(ierr))
+        _check(ierr, "hodlr_b200_factorize_dev")
+        return Factor(out)
+
     def to_host(self) -> Tree:
         t = Tree(self.info()["height"])
         ierr = C.c_int(0)
@@ -271,6 +279,30 @@ class DeviceTree:
     def free(self):
         if self.h:
             lib().hodlr_b200_tree_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Factor:
+    """Handle of a factorised tree (hodlr_b200_factorize_dev)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def solve(self, d_b: int, k: int, ldb: int, d_x: int, ldx: int, stream: int = 0):
+        r = lib().hodlr_b200_solve_dev(self.h, C.c_void_p(d_b), k, ldb, C.c_void_p(d_x), ldx,
+                                       C.c_void_p(stream))
+        if r != abi.SUCCESS:
+            raise HodlrError(r, "hodlr_b200_solve_dev", lib().hodlr_b200_last_error().decode())
+
+    def free(self):
+        if self.h:
+            lib().hodlr_b200_factor_free(self.h)
             self.h = None
 
     def __del__(self):
