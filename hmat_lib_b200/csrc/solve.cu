@@ -2,8 +2,9 @@
 //
 // The capacitance matrix of a node, C = [I, P; Q, I] with P = V_tr^T W2 and
 // Q = V_bl^T W1, has identity diagonal blocks, so only its Schur complement
-// S = I - Q P (order s_bl) is inverted: C^-1 [t1; t2] = [t1 - P y2; y2] with
-// y2 = S^-1 (t2 - Q t1).  Per node the factor keeps P, Q and S^-1.
+// S = I - Q P (order s_bl) is inverted; C^-1 is then assembled from P, Q and
+// S^-1 by two small GEMM launches and kept, so that a solve applies it as one
+// GEMM per level instead of three dependent ones.
 #include <algorithm>
 #include <cmath>
 
@@ -174,143 +175,160 @@ void eye(const std::vector<EyeDesc> &v, cudaStream_t s) {
 int node_index(int d, int j) { return (1 << d) - 1 + j; }
 
 // Base slots of the solver's GEMM launches.
-enum Slot { kS_Arena = 0, kS_Buf = 1, kS_X = 2, kS_T = 3, kS_Y = 4, kS_Tmp = 5 };
+enum Slot { kS_Arena = 0, kS_Buf = 1, kS_X = 2, kS_B = 3, kS_T = 4, kS_Z = 5 };
 
-struct NodeParts {
-  long long p_off, q_off, sinv_off;   // in the factor buffer
+GemmBases solver_bases(const HodlrFactor &f, double *X, const double *B, double *T, double *Z) {
+  GemmBases b{};
+  b.p[kS_Arena] = f.tree->arena;
+  b.p[kS_Buf] = f.buf;
+  b.p[kS_X] = X;
+  b.p[kS_B] = const_cast<double *>(B);
+  b.p[kS_T] = T;
+  b.p[kS_Z] = Z;
+  return b;
+}
+
+// Scratch of one level: t and z of node j at off[j] (q_j x k, ld q_j).
+long long level_scratch(const HodlrFactor &f, int l, int k, std::vector<long long> *off) {
+  long long tot = 0;
+  if (off) off->assign(1 << l, 0);
+  for (int j = 0; j < (1 << l); ++j) {
+    if (off) (*off)[j] = tot;
+    tot += align_up((long long)f.q[node_index(l, j)] * k);
+  }
+  return tot;
+}
+
+// The three launches of x <- (I + W_l V_l^T)^-1 x, x in slot kS_X (ld ldx, k
+// columns), t in kS_T, z in kS_Z.
+struct LevelBatches {
+  GemmBatch vt, cz, wx;
 };
+
+LevelBatches level_batches(const HodlrFactor &f, int l, int k, long long ldx) {
+  const Geometry &g = f.tree->g;
+  std::vector<long long> off;
+  level_scratch(f, l, k, &off);
+  LevelBatches L;
+  const long long wl = f.w_off[l];
+  for (int j = 0; j < (1 << l); ++j) {
+    const BlockDesc &tr = g.blocks[block_index(l, j, 1)], &bl = g.blocks[block_index(l, j, 2)];
+    const int q = tr.s + bl.s;
+    if (q == 0) continue;
+    // t = [V_tr^T x[child 2]; V_bl^T x[child 1]]
+    if (tr.s) {
+      const int p = L.vt.add(kS_T, off[j], q, tr.s, k);
+      L.vt.seg(p, kS_Arena, tr.v_off, tr.n, 1, kS_X, tr.c0, ldx, 0, tr.n);
+    }
+    if (bl.s) {
+      const int p = L.vt.add(kS_T, off[j] + tr.s, q, bl.s, k);
+      L.vt.seg(p, kS_Arena, bl.v_off, bl.n, 1, kS_X, bl.c0, ldx, 0, bl.n);
+    }
+    // z = C^-1 t
+    const int p = L.cz.add(kS_Z, off[j], q, q, k);
+    L.cz.seg(p, kS_Buf, f.cinv_off[node_index(l, j)], q, 0, kS_T, off[j], q, 0, q);
+    // x[child 1] -= W1 z1, x[child 2] -= W2 z2
+    if (tr.s) {
+      const int p1 = L.wx.add(kS_X, tr.r0, ldx, tr.m, k, -1.0, 1.0);
+      L.wx.seg(p1, kS_Buf, wl + tr.r0, g.n, 0, kS_Z, off[j], q, 0, tr.s);
+    }
+    if (bl.s) {
+      const int p2 = L.wx.add(kS_X, bl.r0, ldx, bl.m, k, -1.0, 1.0);
+      L.wx.seg(p2, kS_Buf, wl + bl.r0, g.n, 0, kS_Z, off[j] + tr.s, q, 0, bl.s);
+    }
+  }
+  return L;
+}
+
+// X = D^-1 B: X in slot kS_X, B in kS_B (distinct).
+GemmBatch leaf_batch(const HodlrFactor &f, int k, long long ldb, long long ldx) {
+  const DeviceTree &t = *f.tree;
+  GemmBatch gb;
+  for (int i = 0; i < t.g.nleaf(); ++i) {
+    const LeafDesc &L = t.leaves[i];
+    if (L.m == 0) continue;
+    const int p = gb.add(kS_X, L.r0, ldx, L.m, k);
+    gb.seg(p, kS_Buf, f.leaf_inv_off[i], L.m, 0, kS_B, L.r0, ldb, 0, L.m);
+  }
+  return gb;
+}
+
+constexpr TileShape kShapeLeaves = TileShape::M128N64;
+constexpr TileShape kShapeVt = TileShape::M64N128;
+constexpr TileShape kShapeCz = TileShape::M64N128;
+constexpr TileShape kShapeWx = TileShape::M128N64;
+
+// One-shot application (factorisation, where k is a level's rank).
+void apply_leaves_once(const HodlrFactor &f, const double *B, long long ldb, double *X,
+                       long long ldx, int k, cudaStream_t s) {
+  GemmBatch gb = leaf_batch(f, k, ldb, ldx);
+  gemm_f64_run(gb, solver_bases(f, X, B, nullptr, nullptr), kShapeLeaves, s);
+}
+
+void apply_level_once(const HodlrFactor &f, int l, double *X, int k, long long ldx,
+                      cudaStream_t s) {
+  const long long tot = level_scratch(f, l, k, nullptr);
+  if (tot == 0) return;
+  double *T = dev_alloc(tot, s), *Z = dev_alloc(tot, s);
+  const GemmBases b = solver_bases(f, X, nullptr, T, Z);
+  LevelBatches L = level_batches(f, l, k, ldx);
+  gemm_f64_run(L.vt, b, kShapeVt, s);
+  gemm_f64_run(L.cz, b, kShapeCz, s);
+  gemm_f64_run(L.wx, b, kShapeWx, s, false);
+  dev_free(T, s);
+  dev_free(Z, s);
+}
 
 }  // namespace
 
+struct SolvePlan {
+  GemmPlan leaves;
+  std::vector<std::unique_ptr<GemmPlan>> vt, cz, wx;   // per depth
+  double *T = nullptr, *Z = nullptr;                  // scratch of the largest level
+  ~SolvePlan() {
+    if (T) cudaFree(T);
+    if (Z) cudaFree(Z);
+  }
+};
+
+HodlrFactor::HodlrFactor() = default;
+
 HodlrFactor::~HodlrFactor() {
+  plans.clear();
   if (buf) cudaFree(buf);
 }
 
 namespace {
 
-// Per-node offsets of P, Q, S^-1 (kept beside cinv_off's vector layout).
-struct Layout {
-  std::vector<NodeParts> parts;
-};
-
-// x <- (I + W_l V_l^T)^-1 x for every depth-l node, x with k columns (ld ldx,
-// slot kS_X of `bases`).  Scratch: t (sum (s_tr + s_bl) k) and y (sum s_bl k).
-void apply_level(const HodlrFactor &f, const Layout &L, int l, double *X, int k, long long ldx,
-                 cudaStream_t s) {
-  const DeviceTree &t = *f.tree;
-  const Geometry &g = t.g;
-  std::vector<long long> t_off(1 << l), y_off(1 << l);
-  long long tt = 0, yy = 0;
-  for (int j = 0; j < (1 << l); ++j) {
-    const BlockDesc &tr = g.blocks[block_index(l, j, 1)], &bl = g.blocks[block_index(l, j, 2)];
-    t_off[j] = tt;
-    tt += align_up((long long)(tr.s + bl.s) * k);
-    y_off[j] = yy;
-    yy += align_up((long long)bl.s * k);
-  }
-  if (tt == 0) return;
-  double *T = dev_alloc(tt, s), *Y = dev_alloc(yy, s);
-  GemmBases b{};
-  b.p[kS_Arena] = t.arena;
-  b.p[kS_Buf] = f.buf;
-  b.p[kS_X] = X;
-  b.p[kS_T] = T;
-  b.p[kS_Y] = Y;
-  b.p[kS_Tmp] = T;
-  const long long wl = f.w_off[l];
-  // 1. t1 = V_tr^T x[child 2], t2 = V_bl^T x[child 1]
-  GemmBatch g1;
-  for (int j = 0; j < (1 << l); ++j) {
-    const BlockDesc &tr = g.blocks[block_index(l, j, 1)], &bl = g.blocks[block_index(l, j, 2)];
-    const int q = tr.s + bl.s;
-    if (tr.s) {
-      int p = g1.add(kS_T, t_off[j], q, tr.s, k);
-      g1.seg(p, kS_Arena, tr.v_off, tr.n, 1, kS_X, tr.c0, ldx, 0, tr.n);
-    }
-    if (bl.s) {
-      int p = g1.add(kS_T, t_off[j] + tr.s, q, bl.s, k);
-      g1.seg(p, kS_Arena, bl.v_off, bl.n, 1, kS_X, bl.c0, ldx, 0, bl.n);
-    }
-  }
-  gemm_f64_run(g1, b, TileShape::M64N128, s);
-  // 2. t2 -= Q t1;  3. y = S^-1 t2;  4. t1 -= P y
-  GemmBatch g2, g3, g4;
-  for (int j = 0; j < (1 << l); ++j) {
-    const BlockDesc &tr = g.blocks[block_index(l, j, 1)], &bl = g.blocks[block_index(l, j, 2)];
-    const int q = tr.s + bl.s;
-    const NodeParts &np = L.parts[node_index(l, j)];
-    if (tr.s && bl.s) {
-      int p = g2.add(kS_T, t_off[j] + tr.s, q, bl.s, k, -1.0, 1.0);
-      g2.seg(p, kS_Buf, np.q_off, bl.s, 0, kS_T, t_off[j], q, 0, tr.s);
-    }
-    if (bl.s) {
-      int p = g3.add(kS_Y, y_off[j], bl.s, bl.s, k);
-      g3.seg(p, kS_Buf, np.sinv_off, bl.s, 0, kS_T, t_off[j] + tr.s, q, 0, bl.s);
-    }
-    if (tr.s && bl.s) {
-      int p = g4.add(kS_T, t_off[j], q, tr.s, k, -1.0, 1.0);
-      g4.seg(p, kS_Buf, np.p_off, tr.s, 0, kS_Y, y_off[j], bl.s, 0, bl.s);
-    }
-  }
-  gemm_f64_run(g2, b, TileShape::M64N128, s, false);
-  gemm_f64_run(g3, b, TileShape::M64N128, s, false);
-  gemm_f64_run(g4, b, TileShape::M64N128, s, false);
-  // 5. x[child 1] -= W1 t1, x[child 2] -= W2 y
-  GemmBatch g5;
-  for (int j = 0; j < (1 << l); ++j) {
-    const BlockDesc &tr = g.blocks[block_index(l, j, 1)], &bl = g.blocks[block_index(l, j, 2)];
-    const int q = tr.s + bl.s;
-    if (tr.s) {
-      int p = g5.add(kS_X, tr.r0, ldx, tr.m, k, -1.0, 1.0);
-      g5.seg(p, kS_Buf, wl + tr.r0, g.n, 0, kS_T, t_off[j], q, 0, tr.s);
-    }
-    if (bl.s) {
-      int p = g5.add(kS_X, bl.r0, ldx, bl.m, k, -1.0, 1.0);
-      g5.seg(p, kS_Buf, wl + bl.r0, g.n, 0, kS_Y, y_off[j], bl.s, 0, bl.s);
-    }
-  }
-  gemm_f64_run(g5, b, TileShape::M128N64, s, false);
-  dev_free(T, s);
-  dev_free(Y, s);
+void build_plan(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool split, cudaStream_t s) {
+  if (!batch.empty()) gemm_plan_build(plan, batch, shape, split, s);
 }
 
-// X = D^-1 B, one block-diagonal GEMM launch (X and B distinct).
-void apply_leaves(const HodlrFactor &f, const double *B, long long ldb, double *X, long long ldx,
-                  int k, cudaStream_t s) {
-  const DeviceTree &t = *f.tree;
-  GemmBases b{};
-  b.p[kS_Arena] = t.arena;
-  b.p[kS_Buf] = f.buf;
-  b.p[kS_X] = X;
-  b.p[kS_T] = const_cast<double *>(B);
-  b.p[kS_Y] = X;
-  b.p[kS_Tmp] = X;
-  GemmBatch gb;
-  for (int i = 0; i < t.g.nleaf(); ++i) {
-    const LeafDesc &L = t.leaves[i];
-    if (L.m == 0) continue;
-    int p = gb.add(kS_X, L.r0, ldx, L.m, k);
-    gb.seg(p, kS_Buf, f.dinv_off + f.leaf_inv_off[i], L.m, 0, kS_T, L.r0, ldb, 0, L.m);
+SolvePlan &solve_plan(HodlrFactor &f, int k, long long ldb, long long ldx, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(f.plan_mutex);
+  const auto key = std::make_tuple(k, ldb, ldx, s);
+  auto it = f.plans.find(key);
+  if (it != f.plans.end()) return *it->second;
+  auto P = std::make_unique<SolvePlan>();
+  const int h = f.tree->g.h;
+  GemmBatch lb = leaf_batch(f, k, ldb, ldx);
+  build_plan(P->leaves, lb, kShapeLeaves, true, s);
+  long long scratch = 0;
+  for (int l = 0; l < h; ++l) {
+    scratch = std::max(scratch, level_scratch(f, l, k, nullptr));
+    LevelBatches L = level_batches(f, l, k, ldx);
+    P->vt.push_back(std::make_unique<GemmPlan>());
+    P->cz.push_back(std::make_unique<GemmPlan>());
+    P->wx.push_back(std::make_unique<GemmPlan>());
+    build_plan(*P->vt.back(), L.vt, kShapeVt, true, s);
+    build_plan(*P->cz.back(), L.cz, kShapeCz, true, s);     // K = q: split near the root
+    build_plan(*P->wx.back(), L.wx, kShapeWx, false, s);
   }
-  gemm_f64_run(gb, b, TileShape::M128N64, s);
-}
-
-// The layouts are rebuilt from the factor's geometry when needed.
-Layout layout_of(const HodlrFactor &f) {
-  Layout L;
-  const Geometry &g = f.tree->g;
-  L.parts.resize(g.nblock() / 2 + 1);
-  long long o = f.cinv_off.empty() ? 0 : f.cinv_off[0];
-  for (int d = 0; d < g.h; ++d)
-    for (int j = 0; j < (1 << d); ++j) {
-      const BlockDesc &tr = g.blocks[block_index(d, j, 1)], &bl = g.blocks[block_index(d, j, 2)];
-      NodeParts &np = L.parts[node_index(d, j)];
-      np.p_off = f.cinv_off[node_index(d, j)];
-      np.q_off = np.p_off + align_up((long long)tr.s * bl.s);
-      np.sinv_off = np.q_off + align_up((long long)bl.s * tr.s);
-      (void)o;
-    }
-  return L;
+  HB_CUDA(cudaMalloc(&P->T, sizeof(double) * std::max<long long>(scratch, 1)));
+  HB_CUDA(cudaMalloc(&P->Z, sizeof(double) * std::max<long long>(scratch, 1)));
+  auto &ref = *P;
+  f.plans[key] = std::move(P);
+  return ref;
 }
 
 }  // namespace
@@ -325,7 +343,6 @@ std::unique_ptr<HodlrFactor> hodlr_factorize(std::shared_ptr<DeviceTree> tp, cud
   *status = SUCCESS;
   // ---- layout of the factor buffer ------------------------------------------------
   long long total = 0;
-  f->dinv_off = 0;
   f->leaf_inv_off.resize(g.nleaf());
   for (int i = 0; i < g.nleaf(); ++i) {
     f->leaf_inv_off[i] = total;
@@ -346,14 +363,13 @@ std::unique_ptr<HodlrFactor> hodlr_factorize(std::shared_ptr<DeviceTree> tp, cud
   f->q.assign(nnodes, 0);
   for (int d = 0; d < h; ++d)
     for (int j = 0; j < (1 << d); ++j) {
-      const int s1 = g.blocks[block_index(d, j, 1)].s, s2 = g.blocks[block_index(d, j, 2)].s;
+      const int q = g.blocks[block_index(d, j, 1)].s + g.blocks[block_index(d, j, 2)].s;
       f->cinv_off[node_index(d, j)] = total;
-      f->q[node_index(d, j)] = s1 + s2;
-      total += align_up((long long)s1 * s2) * 2 + align_up((long long)s2 * s2);
+      f->q[node_index(d, j)] = q;
+      total += align_up((long long)q * q);
     }
   HB_CUDA(cudaMalloc(&f->buf, sizeof(double) * std::max<long long>(total, 1)));
   HB_CUDA(cudaMemsetAsync(f->buf, 0, sizeof(double) * std::max<long long>(total, 1), s));
-  const Layout L = layout_of(*f);
   int *d_status = nullptr;
   HB_CUDA(cudaMallocAsync((void **)&d_status, sizeof(int), s));
   HB_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), s));
@@ -365,7 +381,7 @@ std::unique_ptr<HodlrFactor> hodlr_factorize(std::shared_ptr<DeviceTree> tp, cud
       const LeafDesc &lf = t.leaves[i];
       if (lf.m == 0) continue;
       probs.push_back(GjProb{t.arena + lf.off, lf.m, lf.m, nullptr,
-                             f->buf + f->dinv_off + f->leaf_inv_off[i], lf.m});
+                             f->buf + f->leaf_inv_off[i], lf.m});
     }
     gj_inverse(probs, d_status, s);
   }
@@ -388,47 +404,63 @@ std::unique_ptr<HodlrFactor> hodlr_factorize(std::shared_ptr<DeviceTree> tp, cud
     CopyDesc *dcp = upload_tmp(cp, s);
     copy2d_batched(dcp, (int)cp.size(), s);
     cudaFreeAsync(dcp, s);
-    apply_leaves(*f, tmp, n, Wl, n, w, s);
-    for (int lev = h - 1; lev > l; --lev) apply_level(*f, L, lev, Wl, w, n, s);
-    // P = V_tr^T W2, Q = V_bl^T W1, S = I - Q P, S^-1
-    GemmBases b{};
-    b.p[kS_Arena] = t.arena;
-    b.p[kS_Buf] = f->buf;
-    for (int i = 2; i < kGemmBases; ++i) b.p[i] = f->buf;
-    GemmBatch gpq, gs;
-    std::vector<EyeDesc> eyes;
-    std::vector<GjProb> inv;
-    double *S = nullptr;
-    long long stot = 0;
-    std::vector<long long> s_off(1 << l, 0);
+    apply_leaves_once(*f, tmp, n, Wl, n, w, s);
+    for (int lev = h - 1; lev > l; --lev) apply_level_once(*f, lev, Wl, w, n, s);
+
+    // C^-1 of every node of the level.  Scratch per node with both ranks
+    // nonzero: P (s_tr x s_bl), Q (s_bl x s_tr), S (s_bl x s_bl).
+    std::vector<long long> p_off(1 << l, 0), q_off(1 << l, 0), s_off(1 << l, 0);
+    long long scratch = 0;
     for (int j = 0; j < (1 << l); ++j) {
-      const int s2 = g.blocks[block_index(l, j, 2)].s;
-      s_off[j] = stot;
-      stot += align_up((long long)s2 * s2);
+      const int s1 = g.blocks[block_index(l, j, 1)].s, s2 = g.blocks[block_index(l, j, 2)].s;
+      if (!s1 || !s2) continue;
+      p_off[j] = scratch;
+      scratch += align_up((long long)s1 * s2);
+      q_off[j] = scratch;
+      scratch += align_up((long long)s2 * s1);
+      s_off[j] = scratch;
+      scratch += align_up((long long)s2 * s2);
     }
-    S = dev_alloc(stot, s);
-    b.p[kS_Tmp] = S;
+    std::vector<EyeDesc> eyes;
+    for (int j = 0; j < (1 << l); ++j) {
+      const int q = f->q[node_index(l, j)];
+      if (q) eyes.push_back(EyeDesc{f->buf + f->cinv_off[node_index(l, j)], q, q});
+    }
+    eye(eyes, s);                              // C^-1 = I where a rank is zero
+    if (scratch == 0) continue;
+    double *Ps = dev_alloc(scratch, s);
+    const GemmBases b = solver_bases(*f, nullptr, nullptr, Ps, nullptr);
+    GemmBatch gpq, gs, c1, c2;
+    std::vector<EyeDesc> s_eye;
+    std::vector<GjProb> inv;
     for (int j = 0; j < (1 << l); ++j) {
       const BlockDesc &tr = g.blocks[block_index(l, j, 1)], &bl = g.blocks[block_index(l, j, 2)];
-      const NodeParts &np = L.parts[node_index(l, j)];
-      if (tr.s && bl.s) {
-        int p = gpq.add(kS_Buf, np.p_off, tr.s, tr.s, bl.s);          // P: s_tr x s_bl
-        gpq.seg(p, kS_Arena, tr.v_off, tr.n, 1, kS_Buf, f->w_off[l] + bl.r0, n, 0, tr.n);
-        int q = gpq.add(kS_Buf, np.q_off, bl.s, bl.s, tr.s);          // Q: s_bl x s_tr
-        gpq.seg(q, kS_Arena, bl.v_off, bl.n, 1, kS_Buf, f->w_off[l] + tr.r0, n, 0, bl.n);
-        int sp = gs.add(kS_Tmp, s_off[j], bl.s, bl.s, bl.s, -1.0, 1.0);
-        gs.seg(sp, kS_Buf, np.q_off, bl.s, 0, kS_Buf, np.p_off, tr.s, 0, tr.s);
-      }
-      if (bl.s) {
-        eyes.push_back(EyeDesc{S + s_off[j], bl.s, bl.s});
-        inv.push_back(GjProb{S + s_off[j], bl.s, bl.s, nullptr, f->buf + np.sinv_off, bl.s});
-      }
+      const int s1 = tr.s, s2 = bl.s, q = s1 + s2;
+      if (!s1 || !s2) continue;
+      const long long ci = f->cinv_off[node_index(l, j)];
+      const long long br = ci + s1 + (long long)s1 * q, bl_off = ci + s1, tr_off = ci + (long long)s1 * q;
+      int p = gpq.add(kS_T, p_off[j], s1, s1, s2);                 // P = V_tr^T W2
+      gpq.seg(p, kS_Arena, tr.v_off, tr.n, 1, kS_Buf, f->w_off[l] + bl.r0, n, 0, tr.n);
+      p = gpq.add(kS_T, q_off[j], s2, s2, s1);                     // Q = V_bl^T W1
+      gpq.seg(p, kS_Arena, bl.v_off, bl.n, 1, kS_Buf, f->w_off[l] + tr.r0, n, 0, bl.n);
+      p = gs.add(kS_T, s_off[j], s2, s2, s2, -1.0, 1.0);           // S = I - Q P
+      gs.seg(p, kS_T, q_off[j], s2, 0, kS_T, p_off[j], s1, 0, s1);
+      s_eye.push_back(EyeDesc{Ps + s_off[j], s2, s2});
+      inv.push_back(GjProb{Ps + s_off[j], s2, s2, nullptr, f->buf + br, q});   // S^-1 -> C^-1[bl, bl]
+      p = c1.add(kS_Buf, tr_off, q, s1, s2, -1.0);                 // C^-1[tr, bl] = -P S^-1
+      c1.seg(p, kS_T, p_off[j], s1, 0, kS_Buf, br, q, 0, s2);
+      p = c1.add(kS_Buf, bl_off, q, s2, s1, -1.0);                 // C^-1[bl, tr] = -S^-1 Q
+      c1.seg(p, kS_Buf, br, q, 0, kS_T, q_off[j], s2, 0, s2);
+      p = c2.add(kS_Buf, ci, q, s1, s1, -1.0, 1.0);                // C^-1[tr, tr] = I - P C^-1[bl, tr]
+      c2.seg(p, kS_T, p_off[j], s1, 0, kS_Buf, bl_off, q, 0, s2);
     }
     gemm_f64_run(gpq, b, TileShape::M64N128, s);
-    eye(eyes, s);
+    eye(s_eye, s);
     gemm_f64_run(gs, b, TileShape::M64N128, s, false);
     gj_inverse(inv, d_status, s);
-    dev_free(S, s);
+    gemm_f64_run(c1, b, TileShape::M64N128, s, false);
+    gemm_f64_run(c2, b, TileShape::M64N128, s, false);
+    dev_free(Ps, s);
   }
   dev_free(tmp, s);
   int st = 0;
@@ -439,12 +471,17 @@ std::unique_ptr<HodlrFactor> hodlr_factorize(std::shared_ptr<DeviceTree> tp, cud
   return f;
 }
 
-void hodlr_solve(const HodlrFactor &f, const double *B, int k, long long ldb, double *X,
+void hodlr_solve(HodlrFactor &f, const double *B, int k, long long ldb, double *X,
                  long long ldx, cudaStream_t s) {
   if (k <= 0 || f.tree->g.n == 0) return;
-  const Layout L = layout_of(f);
-  apply_leaves(f, B, ldb, X, ldx, k, s);
-  for (int l = f.tree->g.h - 1; l >= 0; --l) apply_level(f, L, l, X, k, ldx, s);
+  SolvePlan &P = solve_plan(f, k, ldb, ldx, s);
+  const GemmBases b = solver_bases(f, X, B, P.T, P.Z);
+  gemm_plan_run(P.leaves, b, s);
+  for (int l = f.tree->g.h - 1; l >= 0; --l) {
+    gemm_plan_run(*P.vt[l], b, s);
+    gemm_plan_run(*P.cz[l], b, s);
+    gemm_plan_run(*P.wx[l], b, s);
+  }
 }
 
 }  // namespace hb

@@ -130,12 +130,14 @@ int hodlr_b200_sync_tree(const struct TreeHODLR *hodlr);
 /* ---- direct solver (no counterpart in hmat_lib) -----------------------------
  * A = D (I + W_{h-1} V_{h-1}^T) ... (I + W_0 V_0^T): leaf inverses, then per
  * depth the level's U blocks solved through the deeper levels and, per node,
- * the inverse of its capacitance matrix's Schur complement (Woodbury).  The
- * factor keeps a reference to the tree.  Factorising returns INPUT_ERROR when
- * a leaf or a capacitance matrix is singular to working precision. */
+ * the inverse of its capacitance matrix (Woodbury).  The factor keeps a
+ * reference to the tree.  Factorising returns INPUT_ERROR when a leaf or a
+ * capacitance matrix is singular to working precision. */
 typedef struct hodlr_b200_factor_s *hodlr_b200_factor;
 int hodlr_b200_factorize_dev(hodlr_b200_tree t, void *stream, hodlr_b200_factor *out, int *ierr);
-/* X = A^-1 B for k right-hand sides (device, column-major; X and B distinct). */
+/* X = A^-1 B for k right-hand sides (device, column-major; X and B distinct).
+ * The first call for a given (k, ldb, ldx, stream) builds and keeps its launch
+ * plans and scratch (synchronously); later calls launch 1 + 3h GEMMs. */
 int hodlr_b200_solve_dev(hodlr_b200_factor f, const double *d_b, int k, int ldb, double *d_x,
                          int ldx, void *stream);
 void hodlr_b200_factor_free(hodlr_b200_factor f);

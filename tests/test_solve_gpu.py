@@ -117,3 +117,29 @@ def test_solve_argument_errors():
     f.free()
     dt.free()
     t.free()
+
+
+def test_cached_plans_for_several_shapes():
+    """Solves with different k and leading dimensions, repeated (the second
+    call of each shape reuses its cached plans and scratch)."""
+    import torch
+    rng = np.random.default_rng(6)
+    sizes = [48, 16, 32, 32, 64, 8, 40, 16]
+    td = _random_tree(sizes, 3, rng, zero_every=4)
+    t = Tree.from_tree_data(td)
+    dt = DeviceTree.of_host(t)
+    f = dt.factorize()
+    n = sum(sizes)
+    a = td.to_dense()
+    for k, ldb, ldx in [(3, n, n), (9, n + 5, n + 2), (3, n, n), (1, n + 1, n), (9, n + 5, n + 2)]:
+        b = rng.standard_normal((ldb, k))
+        bd = torch.from_numpy(np.asfortranarray(b)).cuda().t().contiguous().t()
+        xd = torch.full((ldx, k), float("nan"), dtype=torch.float64).cuda().t().contiguous().t()
+        f.solve(bd.data_ptr(), k, ldb, xd.data_ptr(), ldx)
+        torch.cuda.synchronize()
+        x = xd.cpu().numpy()
+        assert O.rel_fro(x[:n], np.linalg.solve(a, b[:n])) < 1e-11
+        assert np.isnan(x[n:]).all()          # rows past n untouched
+    f.free()
+    dt.free()
+    t.free()
