@@ -15,9 +15,10 @@
 //                        to tmem_full;
 //   warps 2-9            epilogue (two warps per quarter of the TMEM lanes,
 //                        alternate 16-column chunks): wait tmem_full, read the
-//                        S int32 groups of their 32 lanes, recombine in FP64, scale by
-//                        2^(e_r + f_j), release the accumulators (tmem_empty),
-//                        store or atomically add the tile.
+//                        S int32 groups of their 32 lanes, recombine in FP64,
+//                        release the accumulators (tmem_empty), then scale by
+//                        2^(e_r + f_j) and store or atomically add the tile
+//                        while the next tile's MMAs run.
 // The warp also owns the TMEM allocation (512 columns: S groups of <= 64).
 // Every barrier wait is bounded; a wait that runs out sets the CTA's abort
 // flag, every role leaves its loop, the producer waits (bounded) for its
@@ -41,6 +42,13 @@ constexpr size_t kSmem = (size_t)kStages * kStageBytes;        // 221184
 constexpr long long kWaitTries = 1LL << 26;
 constexpr int kSliceBytesA = kOzRowsA * kOzKBlock;              // 4096: one slice of an A block
 
+// int32 -> double, exactly: the double with high word 0x43300000 and low word
+// v + 2^31 is 2^52 + 2^31 + v, so one integer XOR and one subtraction
+// replace the 64-bit conversion instruction.
+__device__ __forceinline__ double exact_double(int32_t v) {
+  return __hiloint2double(0x43300000, (int)((uint32_t)v ^ 0x80000000u)) - 0x1.00000800p52;
+}
+
 // Bounded wait that also gives up when another role has aborted.
 __device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, volatile int *bad) {
   for (long long i = 0; i < kWaitTries; ++i) {
@@ -60,6 +68,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
   __shared__ uint32_t taddr_s;
   __shared__ volatile int bad;
   __shared__ int cexp_s[kEpiWarps][kOzMaxNw];   // per epilogue warp: column exponents of its tile
+  static_assert(kOzSlices == 6, "the epilogue reads the groups in two passes of three");
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 1) {
@@ -198,41 +207,64 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       umma::fence_after_sync();
       const int nw = T.nw;
       const bool row_ok = r < T.rows;
-      const int er = (row_ok ? T.rexp[r] : 0) - 14;
-      double *crow = cbase + T.c_off + r;
-      double rowmax = 0.0;
-      for (int c0 = 16 * half; c0 < nw; c0 += 32) {
-        int32_t v[kOzSlices][16];
+      // sum_t v_t 2^(-7 t) of the (at most two) 16-column chunks of this
+      // warp, held in registers so that the accumulators go back to the MMA
+      // thread before the tile is scaled and stored
+      double acc[2][16];
 #pragma unroll
-        for (int t = 0; t < kOzSlices; ++t) umma::tmem_ld16(lane_addr + t * nw + c0, v[t]);
-        umma::tmem_ld_wait();
-        if (row_ok) {
+      for (int c = 0; c < 2; ++c) {
+        const int c0 = 16 * half + 32 * c;
+        if (c0 < nw) {
+          // two passes of three groups (lowest first) keep 48 int registers
+          // live beside the 32 accumulating doubles
 #pragma unroll
-          for (int x = 0; x < 16; ++x) {
-            const int j = c0 + x;
-            if (j >= T.cols) break;
-            // sum_t v_t 2^(-7 t), then the common factor 2^(e_r + f_j - 14)
-            double acc = (double)v[kOzSlices - 1][x];
+          for (int pass = 0; pass < 2; ++pass) {
+            int32_t v[3][16];
 #pragma unroll
-            for (int t = kOzSlices - 2; t >= 0; --t) acc = fma(acc, 0x1p-7, (double)v[t][x]);
-            const int e = er + cexp_s[ew][j];
-            const double val = (e >= -1022 && e <= 1023)
-                                   ? acc * __longlong_as_double((long long)(e + 1023) << 52)
-                                   : ldexp(acc, e);
-            rowmax = fmax(rowmax, fabs(val));
-            double *c = crow + (long long)j * T.ldc;
-            if (T.atomic)
-              atomicAdd(c, val);
-            else
-              *c = val;
+            for (int u = 0; u < 3; ++u)
+              umma::tmem_ld16(lane_addr + (kOzSlices - 1 - 3 * pass - u) * nw + c0, v[u]);
+            umma::tmem_ld_wait();
+#pragma unroll
+            for (int x = 0; x < 16; ++x) {
+              double a = pass == 0 ? exact_double(v[0][x])
+                                   : fma(acc[c][x], 0x1p-7, exact_double(v[0][x]));
+              a = fma(a, 0x1p-7, exact_double(v[1][x]));
+              acc[c][x] = fma(a, 0x1p-7, exact_double(v[2][x]));
+            }
           }
         }
       }
-      if (T.rmax && row_ok && rowmax > 0.0)
-        atomicMax(T.rmax + r, (unsigned long long)__double_as_longlong(rowmax));
       umma::fence_before_sync();
       __syncwarp();
       if (lane == 0) umma::mbar_arrive(&tmem_empty);
+      // the common factor 2^(e_r + f_j - 14), then store or add
+      if (row_ok) {
+        const int er = T.rexp[r] - 14;
+        double *crow = cbase + T.c_off + r;
+        double rowmax = 0.0;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int c0 = 16 * half + 32 * c;
+#pragma unroll
+          for (int x = 0; x < 16; ++x) {
+            const int j = c0 + x;
+            if (c0 < nw && j < T.cols) {
+              const int e = er + cexp_s[ew][j];
+              const double val = (e >= -1022 && e <= 1023)
+                                     ? acc[c][x] * __longlong_as_double((long long)(e + 1023) << 52)
+                                     : ldexp(acc[c][x], e);
+              rowmax = fmax(rowmax, fabs(val));
+              double *cp = crow + (long long)j * T.ldc;
+              if (T.atomic)
+                atomicAdd(cp, val);
+              else
+                *cp = val;
+            }
+          }
+        }
+        if (T.rmax && rowmax > 0.0)
+          atomicMax(T.rmax + r, (unsigned long long)__double_as_longlong(rowmax));
+      }
     }
   }
 
