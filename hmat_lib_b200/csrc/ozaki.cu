@@ -301,7 +301,7 @@ __device__ __forceinline__ int find_job(const Job *jobs, int njobs, long long it
   return lo;
 }
 
-constexpr int kMaxChunkK = 2048;   // K values per warp item, K-contiguous lines
+constexpr int kMaxChunkK = 1024;   // K values per warp item, K-contiguous lines
 constexpr int kMaxChunkL = 16;     // K values per warp item, line-contiguous (32 lines)
 constexpr int kTileLines = 32;     // shared-memory transpose tile: lines x K values
 constexpr int kTileK = 64;
@@ -330,11 +330,14 @@ __global__ void max_kernel(const MaxJob *__restrict__ jobs, int njobs, long long
       const int k0 = (int)(local % nch) * kMaxChunkK, k1 = min(J.K, k0 + kMaxChunkK);
       const double *row = src + line * J.s_line;
       int k = k0 + lane;
-      for (; k + 96 < k1; k += 128) {
-        m0 = fmax(m0, fabs(row[k]));
-        m1 = fmax(m1, fabs(row[k + 32]));
-        m2 = fmax(m2, fabs(row[k + 64]));
-        m3 = fmax(m3, fabs(row[k + 96]));
+      for (; k + 224 < k1; k += 256) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = row[k + 32 * u];
+        m0 = fmax(m0, fmax(fabs(v[0]), fabs(v[1])));
+        m1 = fmax(m1, fmax(fabs(v[2]), fabs(v[3])));
+        m2 = fmax(m2, fmax(fabs(v[4]), fabs(v[5])));
+        m3 = fmax(m3, fmax(fabs(v[6]), fabs(v[7])));
       }
       for (; k < k1; k += 32) m0 = fmax(m0, fabs(row[k]));
       double mx = fmax(fmax(m0, m1), fmax(m2, m3));
@@ -426,27 +429,62 @@ __global__ void slice_lines_kernel(const SliceJob *__restrict__ jobs, int njobs,
   }
 }
 
+// 8-byte asynchronous copy into shared memory; bytes = 0 writes zeros (the
+// source address is then not read).
+__device__ __forceinline__ void cp_async8z(void *smem, const void *gmem, bool pred) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem),
+               "r"(pred ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_prev() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
+// Stages block item `it` (32 lines x 64 K values) of a K-contiguous slice
+// batch into `buf` with asynchronous copies (zeros outside the source).
+__device__ __forceinline__ void stage_kcontig(const SliceJob *__restrict__ jobs, int njobs,
+                                              long long it, const double *xbase,
+                                              double (*buf)[kTileK + 1]) {
+  const SliceJob &J = jobs[find_job(jobs, njobs, it)];
+  const double *src = J.src ? J.src : xbase;
+  const long long local = it - J.item0;
+  const int Kw = J.nkb * kOzKBlock;
+  const int nkt = (Kw + kTileK - 1) / kTileK;
+  const int line0 = (int)(local / nkt) * kTileLines, k0 = (int)(local % nkt) * kTileK;
+  for (int idx = threadIdx.x; idx < kTileLines * kTileK; idx += blockDim.x) {
+    const int l = idx / kTileK, kk = idx % kTileK;
+    const int line = line0 + l, k = k0 + kk;
+    const bool in = line < J.lines && k < J.K;
+    cp_async8z(&buf[l][kk], in ? src + (long long)line * J.s_line + k : src, in);
+  }
+}
+
 // K-contiguous sources (s_k = 1): one block item = 32 lines x 64 K values,
-// read with coalesced row loads into shared memory, then sliced 16 K values
-// per thread (small tiles keep a dozen blocks resident per SM).
+// brought into shared memory with coalesced asynchronous row copies (the next
+// item's copies in flight while the current one is sliced, two buffers),
+// then sliced 16 K values per thread.
 __global__ void __launch_bounds__(kSliceThreads) slice_kcontig_kernel(const SliceJob *__restrict__ jobs,
                                                             int njobs, long long items,
                                                             const double *xbase) {
-  __shared__ double buf[kTileLines][kTileK + 1];
+  __shared__ double buf[2][kTileLines][kTileK + 1];
   const int tid = threadIdx.x;
-  for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+  long long it = blockIdx.x;
+  if (it < items) stage_kcontig(jobs, njobs, it, xbase, buf[0]);
+  cp_async_commit_group();
+  for (int b = 0; it < items; it += gridDim.x, b ^= 1) {
+    if (it + gridDim.x < items) stage_kcontig(jobs, njobs, it + gridDim.x, xbase, buf[b ^ 1]);
+    cp_async_commit_group();
+    cp_async_wait_prev();            // this item's group has landed
+    __syncthreads();
     const SliceJob &J = jobs[find_job(jobs, njobs, it)];
-    const double *src = J.src ? J.src : xbase;
     const long long local = it - J.item0;
     const int Kw = J.nkb * kOzKBlock;                   // K positions written
     const int nkt = (Kw + kTileK - 1) / kTileK;
     const int line0 = (int)(local / nkt) * kTileLines, k0 = (int)(local % nkt) * kTileK;
-    for (int idx = tid; idx < kTileLines * kTileK; idx += blockDim.x) {
-      const int l = idx / kTileK, kk = idx % kTileK;
-      const int line = line0 + l, k = k0 + kk;
-      buf[l][kk] = (line < J.lines && k < J.K) ? src[(long long)line * J.s_line + k] : 0.0;
-    }
-    __syncthreads();
     const int l = tid % kTileLines, c = tid / kTileLines;   // kTileK / 16 chunks
     const int line = line0 + l, k = k0 + c * 16;
     if (line < J.ntiles * J.R && k < Kw) {
@@ -455,12 +493,12 @@ __global__ void __launch_bounds__(kSliceThreads) slice_kcontig_kernel(const Slic
       if (J.exp_out && k == 0 && live) J.exp_out[line] = ex;
       double y[16];
 #pragma unroll
-      for (int x = 0; x < 16; ++x) y[x] = buf[l][c * 16 + x];
+      for (int x = 0; x < 16; ++x) y[x] = buf[b][l][c * 16 + x];
       const int t = line / J.R, lr = line % J.R;
       slice16(y, ex, J.dst + (long long)t * J.tile_stride +
                          oz_offset(J.R, 0, lr, J.kb0 * kOzKBlock + k), J.R);
     }
-    __syncthreads();
+    __syncthreads();                 // buf[b] is refilled two items later
   }
 }
 
@@ -552,7 +590,8 @@ void ozaki_max(const MaxBatch &b, const double *xbase, cudaStream_t stream) {
 void ozaki_slice(const SliceBatch &b, const double *xbase, cudaStream_t stream) {
   if (b.n <= 0 || b.items <= 0) return;
   if (b.kcontig) {
-    const int grid = (int)std::min<long long>(b.items, (long long)num_sms() * 16);
+    // two 16.6 KB buffers per block: six resident blocks per SM
+    const int grid = (int)std::min<long long>(b.items, (long long)num_sms() * 6);
     slice_kcontig_kernel<<<grid, kSliceThreads, 0, stream>>>(b.d, b.n, b.items, xbase);
   } else {
     slice_lines_kernel<<<grid_for(b.items), 256, 0, stream>>>(b.d, b.n, b.items, xbase);
