@@ -42,11 +42,11 @@ constexpr size_t kSmem = (size_t)kStages * kStageBytes;        // 221184
 constexpr long long kWaitTries = 1LL << 26;
 constexpr int kSliceBytesA = kOzRowsA * kOzKBlock;              // 4096: one slice of an A block
 
-// int32 -> double, exactly: the double with high word 0x43300000 and low word
-// v + 2^31 is 2^52 + 2^31 + v, so one integer XOR and one subtraction
-// replace the 64-bit conversion instruction.
-__device__ __forceinline__ double exact_double(int32_t v) {
-  return __hiloint2double(0x43300000, (int)((uint32_t)v ^ 0x80000000u)) - 0x1.00000800p52;
+// 64-bit integer of magnitude below 2^51 -> double, exactly: adding it to
+// the bit pattern of 1.5 2^52 gives the double 1.5 2^52 + x, so one integer
+// addition and one subtraction replace the 64-bit conversion instruction.
+__device__ __forceinline__ double exact_double46(long long x) {
+  return __longlong_as_double(x + 0x4338000000000000LL) - 0x1.8p52;
 }
 
 // Bounded wait that also gives up when another role has aborted.
@@ -207,9 +207,11 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       umma::fence_after_sync();
       const int nw = T.nw;
       const bool row_ok = r < T.rows;
-      // sum_t v_t 2^(-7 t) of the (at most two) 16-column chunks of this
-      // warp, held in registers so that the accumulators go back to the MMA
-      // thread before the tile is scaled and stored
+      // 2^14 sum_t v_t 2^(-7 t) of the (at most two) 16-column chunks of
+      // this warp, held in registers so that the accumulators go back to the
+      // MMA thread before the tile is scaled and stored.  Each triple of
+      // groups is combined exactly in 64-bit integers (|.| < 2^46), converted
+      // exactly, and the two triples are added with one rounding.
       double acc[2][16];
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
@@ -222,14 +224,14 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
             int32_t v[3][16];
 #pragma unroll
             for (int u = 0; u < 3; ++u)
-              umma::tmem_ld16(lane_addr + (kOzSlices - 1 - 3 * pass - u) * nw + c0, v[u]);
+              umma::tmem_ld16(lane_addr + (3 * (1 - pass) + u) * nw + c0, v[u]);
             umma::tmem_ld_wait();
 #pragma unroll
             for (int x = 0; x < 16; ++x) {
-              double a = pass == 0 ? exact_double(v[0][x])
-                                   : fma(acc[c][x], 0x1p-7, exact_double(v[0][x]));
-              a = fma(a, 0x1p-7, exact_double(v[1][x]));
-              acc[c][x] = fma(a, 0x1p-7, exact_double(v[2][x]));
+              const long long tri =
+                  (long long)v[0][x] * 16384 + (long long)v[1][x] * 128 + (long long)v[2][x];
+              const double d = exact_double46(tri);
+              acc[c][x] = pass == 0 ? d : fma(acc[c][x], 0x1p-21, d);
             }
           }
         }
@@ -237,9 +239,9 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       umma::fence_before_sync();
       __syncwarp();
       if (lane == 0) umma::mbar_arrive(&tmem_empty);
-      // the common factor 2^(e_r + f_j - 14), then store or add
+      // the common factor 2^(e_r + f_j - 28), then store or add
       if (row_ok) {
-        const int er = T.rexp[r] - 14;
+        const int er = T.rexp[r] - 28;
         double *crow = cbase + T.c_off + r;
         double rowmax = 0.0;
 #pragma unroll
