@@ -600,7 +600,8 @@ def main():
         "scaling": "weak", "vs_baseline": None,
         "dtype": "s8 slices -> s32 on tensor cores (6 slices, 21 products), f64 result",
         "data": "synthetic", "precision": "mixed",
-        "config": {"workload": WORKLOAD, "n": n, "height": h, "leaf": n // (1 << h), "k": k,
+        "config": {"workload": WORKLOAD if args.n is None else f"matern2d_n{n}", "n": n,
+                   "height": h, "leaf": n // (1 << h), "k": k,
                    "tol": tol, "kernel": "matern32 l=0.1 +1e-2 I, 2D Morton points seed 1",
                    "l2": "inputs larger than L2 (factors + X > 126 MB), no flush",
                    "parallelism": f"replicas{world}"},

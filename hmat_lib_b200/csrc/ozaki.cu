@@ -1,7 +1,8 @@
 // int8-sliced FP64 products on tcgen05 (see ozaki.h for the scheme and the
 // blocked operand layout).
 //
-// Persistent kernel, one CTA of six warps per SM, tiles taken round-robin:
+// Persistent kernel, one CTA of ten warps per SM, each taking the run of
+// tiles the host schedule gave it (ozaki_schedule):
 //   warp 0               producer: per K-block the A block (all S slices of
 //                        128 lines) and the B block, each as 1-8 bulk copies
 //                        issued by as many lanes, into a six-stage ring,
@@ -26,6 +27,9 @@
 // status 1 and returns.
 #include <algorithm>
 #include <cmath>
+#include <queue>
+#include <utility>
+#include <vector>
 
 #include "ozaki.h"
 #include "umma.cuh"
@@ -59,8 +63,8 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, vo
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
-ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ tiles, int ntiles,
-                  double *cbase, int *status, int split) {
+ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ tiles,
+                  const int *__restrict__ starts, double *cbase, int *status, int split) {
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t empty[kStages];
@@ -90,6 +94,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tbase = taddr_s;
+  const int tile_first = starts[blockIdx.x], tile_end = starts[blockIdx.x + 1];
 
   if (warp == 0) {
     // ---------------- producer ----------------
@@ -97,7 +102,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
     // then each copy 1/split of the A block and of the B block
     long long g = 0;   // K-blocks issued by this CTA
     bool stop = false;
-    for (int tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x) {
+    for (int tile = tile_first; tile < tile_end && !stop; ++tile) {
       stop = __shfl_sync(0xffffffffu, (int)bad, 0) != 0;
       if (stop) break;
       const OzTile T = tiles[tile];
@@ -140,7 +145,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       long long g = 0;
       int lt = 0;
       bool ok = true;
-      for (int tile = blockIdx.x; tile < ntiles && ok && !bad; tile += gridDim.x, ++lt) {
+      for (int tile = tile_first; tile < tile_end && ok && !bad; ++tile, ++lt) {
         const OzTile T = tiles[tile];
         if (lt > 0 && !wait_or_abort(&tmem_empty, (uint32_t)((lt - 1) & 1), &bad)) {
           ok = false;
@@ -192,7 +197,7 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
     const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
     const int r = 32 * quarter + lane;
     int lt = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++lt) {
+    for (int tile = tile_first; tile < tile_end; ++tile, ++lt) {
       if (__any_sync(0xffffffffu, bad)) break;
       const OzTile T = tiles[tile];
       // column exponents of this tile, staged while its MMAs run
@@ -520,21 +525,76 @@ int grid_for(long long threads) {
 
 }  // namespace
 
-void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *cbase,
-                int *d_status, cudaStream_t stream) {
-  if (ntiles <= 0) return;
+int ozaki_grid(int ntiles) { return std::max(0, std::min(ntiles, num_sms())); }
+
+std::vector<int> ozaki_schedule(std::vector<OzTile> &tiles, const std::vector<OzSeg> &segs,
+                                int grid) {
+  std::vector<int> start(grid + 1, 0);
+  if (grid <= 0 || tiles.empty()) {
+    std::fill(start.begin(), start.end(), (int)tiles.size());
+    if (!start.empty()) start[0] = 0;
+    return start;
+  }
+  // cost in K-block x column units; the fixed part is about two K-blocks of
+  // a 64-wide tile (the wait for the accumulators between tiles)
+  constexpr long long kTileCost = 160;
+  std::vector<long long> cost(tiles.size());
+  for (size_t i = 0; i < tiles.size(); ++i) {
+    long long kb = 0;
+    for (int q = tiles[i].seg0; q < tiles[i].seg0 + tiles[i].nseg; ++q) kb += segs[q].nkb;
+    cost[i] = kb * tiles[i].nw + kTileCost;
+  }
+  std::vector<int> order(tiles.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  if (option("ozaki_schedule", 1.0) == 0.0) {
+    // option ozaki_schedule = 0: tile i on CTA i mod grid, in list order
+    std::vector<OzTile> out;
+    out.reserve(tiles.size());
+    for (int b = 0; b < grid; ++b) {
+      start[b] = (int)out.size();
+      for (size_t i = b; i < tiles.size(); i += grid) out.push_back(tiles[i]);
+    }
+    start[grid] = (int)out.size();
+    tiles.swap(out);
+    return start;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  // least-loaded CTA first (ties: lower index)
+  using Slot = std::pair<long long, int>;
+  std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+  for (int b = 0; b < grid; ++b) heap.push({0, b});
+  std::vector<std::vector<int>> owned(grid);
+  for (int i : order) {
+    Slot sl = heap.top();
+    heap.pop();
+    owned[sl.second].push_back(i);
+    heap.push({sl.first + cost[i], sl.second});
+  }
+  std::vector<OzTile> out;
+  out.reserve(tiles.size());
+  for (int b = 0; b < grid; ++b) {
+    start[b] = (int)out.size();
+    for (int i : owned[b]) out.push_back(tiles[i]);
+  }
+  start[grid] = (int)out.size();
+  tiles.swap(out);
+  return start;
+}
+
+void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, const int *d_starts, int grid,
+                double *cbase, int *d_status, cudaStream_t stream) {
+  if (grid <= 0) return;
   static bool configured = false;
   if (!configured) {
     HB_CUDA(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmem));
     configured = true;
   }
-  const int grid = std::min(ntiles, num_sms());
   // bulk copies per operand block (1, 2, 4 or 8 lanes; every chunk stays a
   // multiple of 16 bytes since B blocks are multiples of 384 bytes)
   int split = (int)option("ozaki_copy_split", 1.0);
   split = split >= 8 ? 8 : split >= 4 ? 4 : split >= 2 ? 2 : 1;
-  ozaki_gemm_kernel<<<grid, kThreads, kSmem, stream>>>(d_segs, d_tiles, ntiles, cbase, d_status,
+  ozaki_gemm_kernel<<<grid, kThreads, kSmem, stream>>>(d_segs, d_tiles, d_starts, cbase, d_status,
                                                        split);
   HB_LAUNCHED();
 }

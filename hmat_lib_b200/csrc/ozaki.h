@@ -71,10 +71,22 @@ struct OzTile {
   unsigned long long *rmax;
 };
 
-// Runs all tiles with a persistent grid (one CTA per SM).  `status` (device
+// Persistent grid for a tile list: one CTA per SM, at most one per tile.
+int ozaki_grid(int ntiles);
+
+// Orders `tiles` for a persistent grid of `grid` CTAs and returns where each
+// CTA's run of tiles starts (grid + 1 entries; CTA b takes tiles
+// [start[b], start[b+1])).  Tiles are assigned longest first to the least
+// loaded CTA, a tile's cost being its K-blocks times its width plus a fixed
+// per-tile cost (the accumulator hand-over), so that CTAs finish together.
+// Option ozaki_schedule = 0 gives tile i to CTA i mod grid instead.
+std::vector<int> ozaki_schedule(std::vector<OzTile> &tiles, const std::vector<OzSeg> &segs,
+                                int grid);
+
+// Runs all tiles with the persistent grid of a schedule.  `status` (device
 // int) is set to 1 if a bounded barrier wait ran out.
-void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, int ntiles, double *cbase,
-                int *d_status, cudaStream_t stream);
+void ozaki_gemm(const OzSeg *d_segs, const OzTile *d_tiles, const int *d_starts, int grid,
+                double *cbase, int *d_status, cudaStream_t stream);
 
 // Largest |value| per line of a strided FP64 matrix, element (line, k) at
 // src[line * s_line + k * s_k], combined by atomic max into out[line] (the

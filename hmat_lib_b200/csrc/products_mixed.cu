@@ -108,6 +108,8 @@ struct MixedPlan {
   OzSeg *seg1 = nullptr, *seg2 = nullptr;
   OzTile *tile1 = nullptr, *tile2 = nullptr;
   int ntile1 = 0, ntile2 = 0;
+  int *start1 = nullptr, *start2 = nullptr;   // per-CTA tile runs (ozaki_schedule)
+  int grid1 = 0, grid2 = 0;
   int *status = nullptr;
   // host copies for batches (X jobs with src NULL; phase-1 tiles relative to
   // w, phase-2 tiles relative to Y)
@@ -119,7 +121,7 @@ struct MixedPlan {
     for (void *p : {(void *)xmax, (void *)fmax, (void *)xexp, (void *)fexp, (void *)xa, (void *)xb,
                     (void *)wb, (void *)w, (void *)max_x.d, (void *)max_wsplit.d, (void *)sl_xa.d,
                     (void *)sl_xb.d, (void *)sl_wb.d, (void *)seg1, (void *)seg2, (void *)tile1,
-                    (void *)tile2, (void *)status})
+                    (void *)tile2, (void *)start1, (void *)start2, (void *)status})
       if (p) cudaFree(p);
   }
 };
@@ -405,6 +407,10 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   P.hsx = sx;
   P.hsxb = sxb;
   P.hsb = sb;
+  P.grid1 = ozaki_grid((int)t1s.size());
+  P.grid2 = ozaki_grid((int)t2.size());
+  P.start1 = upload(ozaki_schedule(t1s, s1, P.grid1), s);
+  P.start2 = upload(ozaki_schedule(t2, s2, P.grid2), s);
   P.seg1 = upload(s1, s);
   P.tile1 = upload(t1s, s);
   P.ntile1 = (int)t1s.size();
@@ -435,13 +441,13 @@ void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double 
   HB_CUDA(cudaMemcpyAsync(P.fmax, P.xmax, sizeof(unsigned long long) * k,
                           cudaMemcpyDeviceToDevice, s));
   if (P.w_zero) HB_CUDA(cudaMemsetAsync(P.w, 0, sizeof(double) * P.w_zero, s));
-  ozaki_gemm(P.seg1, P.tile1, P.ntile1, P.w, P.status, s);
+  ozaki_gemm(P.seg1, P.tile1, P.start1, P.grid1, P.w, P.status, s);
   timer.mark(1);
   // 2. common column exponents of X and W, their slices; Y band by band
   ozaki_max(P.max_wsplit, X, s);
   ozaki_slice(P.sl_xb, X, s);
   ozaki_slice(P.sl_wb, X, s);
-  ozaki_gemm(P.seg2, P.tile2, P.ntile2, Y, P.status, s);
+  ozaki_gemm(P.seg2, P.tile2, P.start2, P.grid2, Y, P.status, s);
   timer.mark(2);
 }
 
@@ -456,11 +462,13 @@ struct MixedBatch {
   OzSeg *seg1 = nullptr, *seg2 = nullptr;
   OzTile *tile1 = nullptr, *tile2 = nullptr;
   int ntile1 = 0, ntile2 = 0;
+  int *start1 = nullptr, *start2 = nullptr;   // per-CTA tile runs (ozaki_schedule)
+  int grid1 = 0, grid2 = 0;
   int *status = nullptr;
   ~MixedBatch() {
     for (void *p : {(void *)pre, (void *)mid, (void *)max_x.d, (void *)max_w.d, (void *)sl_xa.d,
                     (void *)sl_xb.d, (void *)sl_wb.d, (void *)seg1, (void *)seg2, (void *)tile1,
-                    (void *)tile2, (void *)status})
+                    (void *)tile2, (void *)start1, (void *)start2, (void *)status})
       if (p) cudaFree(p);
   }
 };
@@ -544,6 +552,10 @@ std::unique_ptr<MixedBatch, MixedBatchDeleter> mixed_batch_build(const std::vect
   B->sl_xa = ozaki_slice_batch(sx, s);
   B->sl_xb = ozaki_slice_batch(sxb, s);
   B->sl_wb = ozaki_slice_batch(sb, s);
+  B->grid1 = ozaki_grid((int)t1s.size());
+  B->grid2 = ozaki_grid((int)t2.size());
+  B->start1 = upload(ozaki_schedule(t1s, s1, B->grid1), s);
+  B->start2 = upload(ozaki_schedule(t2, s2, B->grid2), s);
   B->seg1 = upload(s1, s);
   B->seg2 = upload(s2, s);
   B->tile1 = upload(t1s, s);
@@ -561,11 +573,11 @@ void mixed_batch_run(MixedBatch &B, cudaStream_t s) {
   ozaki_max(B.max_x, nullptr, s);
   ozaki_slice(B.sl_xa, nullptr, s);
   ozaki_ranges(B.mid, B.nmid, s);
-  ozaki_gemm(B.seg1, B.tile1, B.ntile1, B.base, B.status, s);
+  ozaki_gemm(B.seg1, B.tile1, B.start1, B.grid1, B.base, B.status, s);
   ozaki_max(B.max_w, nullptr, s);
   ozaki_slice(B.sl_xb, nullptr, s);
   ozaki_slice(B.sl_wb, nullptr, s);
-  ozaki_gemm(B.seg2, B.tile2, B.ntile2, B.base, B.status, s);
+  ozaki_gemm(B.seg2, B.tile2, B.start2, B.grid2, B.base, B.status, s);
 }
 
 int mixed_batch_status(MixedBatch &B, cudaStream_t s) {
