@@ -1,4 +1,5 @@
 // Device tree arena, upload / download and the host-tree registry.
+#include <atomic>
 #include <cstring>
 #include <unordered_map>
 
@@ -33,13 +34,45 @@ cudaStream_t lib_stream() {
   HB_CUDA(cudaGetDevice(&dev));
   auto it = streams.find(dev);
   if (it != streams.end()) return it->second;
+  keep_pool_memory();
   cudaStream_t s;
   HB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   streams[dev] = s;
   return s;
 }
 
+// Freed stream-ordered memory stays mapped in the device's default pool
+// (release threshold unlimited), so that a build, whose sketch rounds
+// synchronise with the host, does not unmap its scratch at every
+// synchronisation and map it again in the next round.  Option pool_keep = 0,
+// set before the library's first allocation on a device, leaves the pool as
+// the process configured it.  Applied once per device.
+void keep_pool_memory() {
+  static std::atomic<unsigned long long> done{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    (void)cudaGetLastError();
+    return;
+  }
+  const unsigned long long bit = 1ULL << dev;
+  if (done.load(std::memory_order_acquire) & bit) return;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.load() & bit) return;
+  done.fetch_or(bit);
+  if (option("pool_keep", 1.0) == 0.0) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  uint64_t keep = ~0ULL;
+  if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+    (void)cudaGetLastError();
+}
+
 double *dev_alloc(size_t elems, cudaStream_t stream) {
+  keep_pool_memory();
   void *p = nullptr;
   HB_CUDA(cudaMallocAsync(&p, std::max<size_t>(elems, 1) * sizeof(double), stream));
   return (double *)p;

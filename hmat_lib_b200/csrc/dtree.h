@@ -60,6 +60,9 @@ void register_device_tree(const TreeHODLR *t, std::shared_ptr<DeviceTree> dt);
 cudaStream_t lib_stream();
 
 // Stream-ordered scratch allocation.
+// Keeps freed stream-ordered memory mapped in the current device's default
+// pool (once per device; option pool_keep).
+void keep_pool_memory();
 double *dev_alloc(size_t elems, cudaStream_t stream);
 void dev_free(void *p, cudaStream_t stream);
 

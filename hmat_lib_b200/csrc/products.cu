@@ -139,9 +139,12 @@ namespace {
 std::mutex g_pt_mutex;
 struct PhaseEvents {
   cudaEvent_t e[3];
+  cudaEvent_t k[4];   // around the GEMM launch of each phase, when marked
+  bool kmarks;
 };
 std::vector<PhaseEvents> g_pending;
 double g_phase_ms[2] = {0.0, 0.0};
+double g_kernel_ms[2] = {0.0, 0.0};
 long long g_phase_count = 0;
 
 void collect_phase_times() {
@@ -152,8 +155,19 @@ void collect_phase_times() {
     cudaEventElapsedTime(&b, pe.e[1], pe.e[2]);
     g_phase_ms[0] += a;
     g_phase_ms[1] += b;
+    if (pe.kmarks) {
+      float c = 0.f, d = 0.f;
+      cudaEventElapsedTime(&c, pe.k[0], pe.k[1]);
+      cudaEventElapsedTime(&d, pe.k[2], pe.k[3]);
+      g_kernel_ms[0] += c;
+      g_kernel_ms[1] += d;
+    } else {            // the phase is its GEMM launch
+      g_kernel_ms[0] += a;
+      g_kernel_ms[1] += b;
+    }
     g_phase_count += 1;
     for (auto ev : pe.e) cudaEventDestroy(ev);
+    for (auto ev : pe.k) cudaEventDestroy(ev);
   }
   g_pending.clear();
 }
@@ -163,7 +177,14 @@ PhaseTimer::PhaseTimer(cudaStream_t s) : stream(s) {
   on = option("record_phase_times", 0.0) != 0.0;
   if (!on) return;
   for (auto &ev : e) HB_CUDA(cudaEventCreate(&ev));
+  for (auto &ev : k) HB_CUDA(cudaEventCreate(&ev));
   HB_CUDA(cudaEventRecord(e[0], stream));
+}
+
+void PhaseTimer::kernel(int phase, bool end) {
+  if (!on) return;
+  kmarks = true;
+  HB_CUDA(cudaEventRecord(k[2 * (phase - 1) + (end ? 1 : 0)], stream));
 }
 
 void PhaseTimer::mark(int i) {
@@ -171,7 +192,7 @@ void PhaseTimer::mark(int i) {
   HB_CUDA(cudaEventRecord(e[i], stream));
   if (i == 2) {
     std::lock_guard<std::mutex> lk(g_pt_mutex);
-    g_pending.push_back(PhaseEvents{{e[0], e[1], e[2]}});
+    g_pending.push_back(PhaseEvents{{e[0], e[1], e[2]}, {k[0], k[1], k[2], k[3]}, kmarks});
   }
 }
 
@@ -181,9 +202,12 @@ int phase_times(double *out, int cap) {
   if (cap >= 1 && out) out[0] = g_phase_ms[0];
   if (cap >= 2 && out) out[1] = g_phase_ms[1];
   if (cap >= 3 && out) out[2] = (double)g_phase_count;
+  if (cap >= 4 && out) out[3] = g_kernel_ms[0];
+  if (cap >= 5 && out) out[4] = g_kernel_ms[1];
   g_phase_ms[0] = g_phase_ms[1] = 0.0;
+  g_kernel_ms[0] = g_kernel_ms[1] = 0.0;
   g_phase_count = 0;
-  return 3;
+  return 5;
 }
 
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,

@@ -86,18 +86,25 @@ std::string batched_tuning();    // configuration the autotuner chose for the la
 void batched_release();          // drops every cached batch plan
 
 // Events around the two phases of a product when option
-// "record_phase_times" is set (mark(1) after phase 1, mark(2) at the end).
+// "record_phase_times" is set (mark(1) after phase 1, mark(2) at the end),
+// and optionally around the main GEMM launch of each phase (kernel(p, false)
+// just before it, kernel(p, true) just after) when a phase also runs other
+// kernels.
 struct PhaseTimer {
   cudaStream_t stream;
   bool on = false;
+  bool kmarks = false;
   cudaEvent_t e[3] = {};
+  cudaEvent_t k[4] = {};
   explicit PhaseTimer(cudaStream_t s);
+  void kernel(int phase, bool end);
   void mark(int i);
 };
 
 // Accumulated per-phase device times (ms) of products run with option
-// "record_phase_times" set: out[0] phase 1, out[1] phase 2, out[2] count.
-// Resets the accumulators.
+// "record_phase_times" set: out[0] phase 1, out[1] phase 2, out[2] count,
+// out[3] / out[4] the GEMM launch of phase 1 / 2 alone.  Resets the
+// accumulators.
 int phase_times(double *out, int cap);
 
 // Base slots and element offsets of one product's operands inside a GEMM

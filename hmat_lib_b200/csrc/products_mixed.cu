@@ -441,13 +441,17 @@ void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double 
   HB_CUDA(cudaMemcpyAsync(P.fmax, P.xmax, sizeof(unsigned long long) * k,
                           cudaMemcpyDeviceToDevice, s));
   if (P.w_zero) HB_CUDA(cudaMemsetAsync(P.w, 0, sizeof(double) * P.w_zero, s));
+  timer.kernel(1, false);
   ozaki_gemm(P.seg1, P.tile1, P.start1, P.grid1, P.w, P.status, s);
+  timer.kernel(1, true);
   timer.mark(1);
   // 2. common column exponents of X and W, their slices; Y band by band
   ozaki_max(P.max_wsplit, X, s);
   ozaki_slice(P.sl_xb, X, s);
   ozaki_slice(P.sl_wb, X, s);
+  timer.kernel(2, false);
   ozaki_gemm(P.seg2, P.tile2, P.start2, P.grid2, Y, P.status, s);
+  timer.kernel(2, true);
   timer.mark(2);
 }
 

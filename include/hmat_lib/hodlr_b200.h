@@ -39,7 +39,11 @@ enum HodlrB200Precision {
 const char *hodlr_b200_version(void);
 /* Message describing the last failure on the calling thread. */
 const char *hodlr_b200_last_error(void);
-/* Runtime knobs, e.g. "jacobi_max_sweeps". Returns SUCCESS. */
+/* Runtime knobs, e.g. "jacobi_max_sweeps". Returns SUCCESS.  "pool_keep"
+ * (default 1): freed stream-ordered scratch stays mapped in the device's
+ * default memory pool (release threshold unlimited) instead of being returned
+ * at every synchronisation; set it to 0 before the library's first call on a
+ * device to leave that pool's configuration untouched. */
 int hodlr_b200_set_option(const char *name, double value);
 /* Allocator for every host buffer the library allocates (tree nodes, factor
  * copies, results returned for out == NULL).  Both NULL restores malloc/free. */
@@ -99,7 +103,10 @@ int hodlr_b200_kernel_matrix_dev(const double *d_points, int n, int dim, int kin
 /* Device time (ms) of the two product phases accumulated since the last call
  * while option "record_phase_times" is non-zero: out[0] projections
  * (W = V^T X), out[1] output bands (Y = D X + sum U W), out[2] number of
- * products.  Resets the accumulators; returns the number of values. */
+ * products, out[3] / out[4] the main GEMM launch of each phase alone (for
+ * mixed products the phases also slice their operands; for FP64 products
+ * these equal out[0] / out[1]).  Resets the accumulators; returns the
+ * number of values. */
 int hodlr_b200_phase_times(double *out, int capacity);
 /* Statistics of the calling thread's most recent build: exact blocks,
  * sketched blocks, sketch rounds, seconds, cap hit, max Jacobi sweeps (exact,
