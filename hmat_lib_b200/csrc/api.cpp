@@ -89,23 +89,95 @@ void d2h(double *dst, long long ld, const double *src, long long rows, long long
                             rows * sizeof(double), cols, cudaMemcpyDeviceToHost, s));
 }
 
+// Copy streams of the host-buffer products (0: host to device, 1: device to
+// host), one pair per device and thread like the library stream.
+cudaStream_t copy_stream(int which) {
+  static thread_local std::map<std::pair<int, int>, cudaStream_t> streams;
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_pair(dev, which);
+  auto it = streams.find(key);
+  if (it != streams.end()) return it->second;
+  cudaStream_t st;
+  HB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  streams[key] = st;
+  return st;
+}
+
+struct Events {
+  std::vector<cudaEvent_t> e;
+  explicit Events(size_t n) : e(n, nullptr) {
+    for (auto &ev : e) HB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  ~Events() {
+    for (auto ev : e)
+      if (ev) cudaEventDestroy(ev);
+  }
+};
+
 // Host-buffer product shared by multiply_vector / multiply_*_dense.
-// X is xr x xc (ld ldx); Y has the same shape (ld ldy).
+// X is xr x xc (ld ldx); Y has the same shape (ld ldy).  The columns of H X
+// and H^T X are independent, so with 128 columns or more the call runs in up
+// to four column chunks: chunk c + 1 is copied in while chunk c is multiplied
+// and chunk c - 1 copied out (two copy streams and the library stream, ordered
+// by events; with pinned host buffers the PCIe transfers in both directions
+// overlap the products).  Option host_chunks = 1 runs the call in one piece;
+// a larger value sets the number of chunks.
 void host_product(DeviceTree &t, ProdOp op, const double *X, long long xr, long long xc,
                   long long ldx, double *Y, long long ldy) {
   cudaStream_t s = lib_stream();
   DevBuf dx(xr * xc, s), dy(xr * xc, s);
-  h2d(dx.p, X, xr, xc, ldx, s);
-  const int k = (int)(op == ProdOp::L ? xr : xc);
   // option "matmat_precision" = 1 routes H X through the int8 tensor-core
   // path (about 42 bits); the default keeps FP64 throughout
   bool aligned = true;
   for (int m : t.g.leaf_m) aligned = aligned && (m % 32 == 0);
-  if (op == ProdOp::N && aligned && option("matmat_precision", 0.0) == 1.0)
-    product_mixed(t, dx.p, k, xr, dy.p, xr, s);
-  else
-    product_f64(t, op, dx.p, k, xr, dy.p, xr, s);
-  d2h(Y, ldy, dy.p, xr, xc, s);
+  const bool mixed = op == ProdOp::N && aligned && option("matmat_precision", 0.0) == 1.0;
+  auto product = [&](const double *xd, double *yd, int k) {
+    if (mixed)
+      product_mixed(t, xd, k, xr, yd, xr, s);
+    else
+      product_f64(t, op, xd, k, xr, yd, xr, s);
+  };
+  long long chunks = (op != ProdOp::L && xc >= 128) ? std::min<long long>(4, xc / 64) : 1;
+  const double opt = option("host_chunks", 0.0);
+  if (opt >= 1.0 && op != ProdOp::L) chunks = std::max(1LL, std::min((long long)opt, xc));
+  if (chunks <= 1 || xr == 0) {
+    h2d(dx.p, X, xr, xc, ldx, s);
+    product(dx.p, dy.p, (int)(op == ProdOp::L ? xr : xc));
+    d2h(Y, ldy, dy.p, xr, xc, s);
+    HB_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
+  cudaStream_t si = copy_stream(0), so = copy_stream(1);
+  Events ev(2 * chunks + 2);
+  cudaEvent_t *in = ev.e.data(), *done = ev.e.data() + chunks;
+  cudaEvent_t allocated = ev.e[2 * chunks], copied_out = ev.e[2 * chunks + 1];
+  // the buffers are stream-ordered allocations of s
+  HB_CUDA(cudaEventRecord(allocated, s));
+  HB_CUDA(cudaStreamWaitEvent(si, allocated, 0));
+  HB_CUDA(cudaStreamWaitEvent(so, allocated, 0));
+  const long long per = (xc + chunks - 1) / chunks;
+  try {
+    for (long long c = 0; c < chunks; ++c) {
+      const long long c0 = c * per, c1 = std::min(xc, c0 + per);
+      if (c0 >= c1) break;
+      h2d(dx.p + c0 * xr, X + c0 * ldx, xr, c1 - c0, ldx, si);
+      HB_CUDA(cudaEventRecord(in[c], si));
+      HB_CUDA(cudaStreamWaitEvent(s, in[c], 0));
+      product(dx.p + c0 * xr, dy.p + c0 * xr, (int)(c1 - c0));
+      HB_CUDA(cudaEventRecord(done[c], s));
+      HB_CUDA(cudaStreamWaitEvent(so, done[c], 0));
+      d2h(Y + c0 * ldy, ldy, dy.p + c0 * xr, xr, c1 - c0, so);
+    }
+  } catch (...) {
+    // no copy may still use the buffers when they are freed
+    cudaStreamSynchronize(si);
+    cudaStreamSynchronize(so);
+    throw;
+  }
+  // the buffers are freed on s after the last copy out
+  HB_CUDA(cudaEventRecord(copied_out, so));
+  HB_CUDA(cudaStreamWaitEvent(s, copied_out, 0));
   HB_CUDA(cudaStreamSynchronize(s));
 }
 

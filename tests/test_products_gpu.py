@@ -184,3 +184,48 @@ def test_large_product_against_dense():
     dense = td.to_dense()
     assert O.rel_fro(t.matmat(x, "N"), dense @ x) < 1e-12
     assert O.rel_fro(t.matmat(x, "T"), dense.T @ x) < 1e-12
+
+
+@pytest.mark.parametrize("chunks", [0, 1, 3, 7])
+def test_host_products_in_column_chunks(lib, chunks):
+    """multiply_hodlr_dense / multiply_hodlr_transpose_dense with host
+    buffers run in column chunks whose copies overlap the products (option
+    host_chunks: 0 automatic, 1 one piece, more: that many chunks); every
+    chunking gives the oracle's result and leaves the rows past n of the
+    output untouched."""
+    n, h, k, ldx, ldy = 1000, 3, 200, 1013, 1007
+    td = random_tree(n, h, seed=11)
+    t = Tree.from_tree_data(td)
+    x = np.asfortranarray(np.random.default_rng(12).standard_normal((ldx, k)))
+    ierr = C.c_int(-1)
+    lib.hodlr_b200_set_option(b"host_chunks", float(chunks))
+    try:
+        for fn, ref in [(lib.multiply_hodlr_dense, O.multiply_dense),
+                        (lib.multiply_hodlr_transpose_dense, O.multiply_transpose_dense)]:
+            y = np.full((ldy, k), np.nan, order="F")
+            assert fn(t.tp, x.ctypes.data_as(abi.DP), k, ldx, y.ctypes.data_as(abi.DP), ldy,
+                      C.byref(ierr))
+            assert ierr.value == abi.SUCCESS
+            assert O.rel_fro(y[:n], ref(td, np.ascontiguousarray(x[:n]))) < REL
+            assert np.isnan(y[n:]).all()
+    finally:
+        lib.hodlr_b200_set_option(b"host_chunks", 0.0)
+    t.free()
+
+
+def test_host_mixed_product_in_column_chunks(lib):
+    """The mixed-precision host product (option matmat_precision = 1) in
+    automatic column chunks agrees with the FP64 one to 1e-11."""
+    n, h, k = 1024, 3, 256
+    td = random_tree(n, h, seed=13)
+    t = Tree.from_tree_data(td)
+    x = np.asfortranarray(np.random.default_rng(14).standard_normal((n, k)))
+    y64 = t.matmat(x, "N")
+    lib.hodlr_b200_set_option(b"matmat_precision", 1.0)
+    try:
+        ymx = t.matmat(x, "N")
+    finally:
+        lib.hodlr_b200_set_option(b"matmat_precision", 0.0)
+    assert O.rel_fro(ymx, y64) < 1e-11
+    assert O.rel_fro(y64, O.multiply_dense(td, x)) < REL
+    t.free()
