@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--n", type=int, default=None, help="override n (testing only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=4096)
+    ap.add_argument("--no-side", action="store_true",
+                    help="skip the n = 1024 H x and n = 16384 H x H measurements")
     ap.add_argument("--batch", type=int, default=512,
                     help="instances of the uneven-batch measurement (0: skip)")
     return ap.parse_args()
@@ -178,6 +180,105 @@ def build_stats(lib):
             "largest_sketch": int(st[9]), "ms_small_svd": st[10], "ms_rounds": st[11],
             "ms_core_svd": st[12], "ms_finish": st[13], "learned_fallbacks": int(st[14]),
             "ms_features": st[15]}
+
+
+def side_workloads(lib, torch, dev, stream, sh):
+    """The two smaller workloads of the hot path, measured beside the main
+    one: H x on the n = 1024 Gaussian tree (exp(-r^2 / (2 0.2^2)) + I on
+    sorted 1D points, seed 0, depth 3, tol 1e-10), device-resident, against
+    the dense product; and H_A H_B on n = 16384 (Gaussian l = 0.1 and
+    Matern-3/2 l = 0.2, both + I, sorted 1D points seed 3, depth 7, tol 1e-8),
+    its time and its error against A (B X) with the dense kernel matrices
+    (X: 16 columns of N(0,1)).  Both trees are built from their points on the
+    device."""
+    from hmat_lib_b200 import workloads as W
+    from hmat_lib_b200.hodlr import DeviceTree
+    kinds = {"gaussian": 0, "matern32": 1, "exponential": 2}
+
+    def dense(d_pts, n, kind, length, diag):
+        a = torch.empty(n * n, dtype=torch.float64, device=dev)
+        assert lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, 1, kinds[kind],
+                                                length, diag, C.c_void_p(a.data_ptr()), n,
+                                                C.c_void_p(sh)) == 0
+        return a.view(n, n)          # row-major view of the symmetric matrix
+
+    out = {}
+    with torch.cuda.stream(stream):
+        # ---- H x, n = 1024
+        w = W.WORKLOADS["gauss1d_n1024"]
+        n = w["n"]
+        d_pts = torch.from_numpy(W.workload_points("gauss1d_n1024").reshape(-1).copy()).to(dev)
+        t = DeviceTree.build_kernel(d_pts.data_ptr(), n, 1, kinds[w["kind"]], w["length"],
+                                    w["diag"], w["height"], w["tol"], stream=sh)
+        x = torch.randn(n, dtype=torch.float64, device=dev)
+        y = torch.zeros_like(x)
+        for _ in range(20):
+            t.matmat(x.data_ptr(), 1, n, y.data_ptr(), n, stream=sh)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 500
+        e0.record(stream)
+        for _ in range(reps):
+            t.matmat(x.data_ptr(), 1, n, y.data_ptr(), n, stream=sh)
+        e1.record(stream)
+        stream.synchronize()
+        a = dense(d_pts, n, w["kind"], w["length"], w["diag"])
+        yd = a @ x
+        stream.synchronize()
+        info = t.info()
+        ms = e0.elapsed_time(e1) / reps
+        out["matvec_n1024"] = {
+            "us_per_matvec": ms * 1e3, "height": w["height"], "tol": w["tol"],
+            "GB_per_s": (8.0 * info["storage"] + 16.0 * n) / (ms * 1e-3) / 1e9,
+            "rel_err_vs_dense": (torch.linalg.norm(y - yd) / torch.linalg.norm(yd)).item(),
+            "note": "device-resident FP64 H x; launch-latency bound at this size"}
+        t.free()
+        del a
+        # ---- H_A H_B, n = 16384
+        n, h, tol = 16384, 7, 1e-8
+        pts, ka, kb = W.hxh_pair(n, seed=3)
+        d_pts = torch.from_numpy(pts.reshape(-1).copy()).to(dev)
+        ta = DeviceTree.build_kernel(d_pts.data_ptr(), n, 1, kinds[ka[0]], ka[1], ka[2], h, tol,
+                                     stream=sh)
+        tb = DeviceTree.build_kernel(d_pts.data_ptr(), n, 1, kinds[kb[0]], kb[1], kb[2], h, tol,
+                                     stream=sh)
+        stream.synchronize()
+        tc = ta.hxh(tb, tol)                      # warm-up (kernels loaded, pool grown)
+        tc.free()
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            tc = ta.hxh(tb, tol)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            if len(times) < 3:
+                tc.free()
+        xk = torch.randn(16, n, dtype=torch.float64, device=dev)     # column-major n x 16
+        yc = torch.zeros_like(xk)
+        tc.matmat(xk.data_ptr(), 16, n, yc.data_ptr(), n, stream=sh)
+        ab = torch.zeros_like(xk)
+        tb.matmat(xk.data_ptr(), 16, n, ab.data_ptr(), n, stream=sh)
+        yh = torch.zeros_like(xk)
+        ta.matmat(ab.data_ptr(), 16, n, yh.data_ptr(), n, stream=sh)
+        stream.synchronize()
+        da = dense(d_pts, n, *ka)
+        db = dense(d_pts, n, *kb)
+        yd = (xk @ db) @ da                        # rows of (A (B X))^T; A, B symmetric
+        stream.synchronize()
+        cinfo = tc.info()
+        out["hxh_n16384"] = {
+            "seconds": min(times), "height": h, "tol": tol,
+            "max_rank_out": cinfo["max_rank"],
+            "rel_err_vs_dense": (torch.linalg.norm(yc - yd) / torch.linalg.norm(yd)).item(),
+            "rel_err_vs_factors_product": (torch.linalg.norm(yc - yh) / torch.linalg.norm(yh)).item(),
+            "check": "(H_A H_B) X vs A (B X) with the dense kernel matrices, X n x 16"}
+        tc.free()
+        ta.free()
+        tb.free()
+        del da, db
+    torch.cuda.empty_cache()
+    return out
 
 
 def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, rank=0, world=1):
@@ -507,6 +608,9 @@ def main():
     fac.free()
     del xs, r_solve
 
+    # ---- the smaller workloads: H x at n = 1024, H x H at n = 16384 -----------------
+    side = side_workloads(lib, torch, dev, stream, sh) if not args.no_side else {}
+
     # ---- e2e through the C-ABI with host buffers ------------------------------------
     host_tree = tree.to_host()
     xh = torch.randn(k, n, dtype=torch.float64).pin_memory()
@@ -632,6 +736,7 @@ def main():
         "rel_err_vs_dense": rel_err,
         "rel_err_mixed_vs_fp64": rel_err_mixed_vs_fp64,
         "solve": solve_info,
+        **side,
         "tree": {"max_rank": info["max_rank"], "storage_doubles": storage,
                  "ranks_by_depth": [int(max(ranks[2 * ((1 << d) - 1):2 * ((1 << (d + 1)) - 1)]))
                                     for d in range(h)]},

@@ -19,6 +19,8 @@ DeviceTree::~DeviceTree() {
   if (arena) cudaFree(arena);
   if (d_leaves) cudaFree(d_leaves);
   if (d_blocks) cudaFree(d_blocks);
+  if (mv_woff) cudaFree(mv_woff);
+  if (mv_w) cudaFree(mv_w);
 }
 
 long long DeviceTree::storage() const {

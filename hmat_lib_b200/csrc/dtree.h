@@ -29,6 +29,8 @@ struct DeviceTree {
   std::map<std::tuple<int, int, long long, long long, int, int>, std::unique_ptr<ProductPlan>> plans;
   std::mutex plan_mutex;
   std::shared_ptr<MixedState> mixed;   // int8 slices of the factors (mixed precision)
+  int *mv_woff = nullptr;              // single-vector product: W offset of every block
+  double *mv_w = nullptr;              // and W (made on the first such product)
 
   DeviceTree() = default;
   DeviceTree(const DeviceTree &) = delete;

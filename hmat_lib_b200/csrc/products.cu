@@ -213,6 +213,15 @@ int phase_times(double *out, int cap) {
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
                  long long ldy, cudaStream_t stream, int min_depth) {
   if (k <= 0 || t.g.n == 0) return;
+  // one vector: the HBM-bound matvec kernels (option matvec_kernels = 0 keeps
+  // the GEMM engine)
+  if (k == 1 && op == ProdOp::N && min_depth == 0 && option("matvec_kernels", 1.0) != 0.0) {
+    PhaseTimer timer(stream);
+    matvec_f64(t, X, Y, stream);
+    timer.mark(1);
+    timer.mark(2);
+    return;
+  }
   ProductPlan &plan = product_plan(t, op, k, ldx, ldy, stream, min_depth);
   GemmBases bases{};
   bases.p[kArena] = t.arena;

@@ -107,6 +107,10 @@ struct PhaseTimer {
 // accumulators.
 int phase_times(double *out, int cap);
 
+// y = H x for one vector (op N) by the dedicated projection and row kernels
+// (matvec.cu); y and x distinct, both of length n.
+void matvec_f64(DeviceTree &t, const double *x, double *y, cudaStream_t stream);
+
 // Base slots and element offsets of one product's operands inside a GEMM
 // batch: a single tree uses its own slots with zero offsets; a batch of trees
 // addresses every operand from one common base.

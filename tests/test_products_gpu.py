@@ -229,3 +229,24 @@ def test_host_mixed_product_in_column_chunks(lib):
     assert O.rel_fro(ymx, y64) < 1e-11
     assert O.rel_fro(y64, O.multiply_dense(td, x)) < REL
     t.free()
+
+
+@pytest.mark.parametrize("use_kernels", [1, 0])
+def test_single_vector_products(lib, use_kernels):
+    """One right-hand side (multiply_vector and H X with k = 1) goes through
+    the dedicated projection and row kernels (option matvec_kernels = 1, the
+    default) or the GEMM engine (0); both match the oracle on uneven leaves
+    with zero-rank blocks and on a depth-5 tree."""
+    lib.hodlr_b200_set_option(b"matvec_kernels", float(use_kernels))
+    try:
+        for ms, h, seed in [([3, 1, 7, 2, 9, 4, 1, 5], 3, 21), (None, 5, 22)]:
+            n = sum(ms) if ms else 2000
+            td = random_tree(n, h, seed=seed, ms=ms, zero_rank_every=3)
+            t = Tree.from_tree_data(td)
+            x = np.random.default_rng(seed).standard_normal(n)
+            want = O.multiply_dense(td, x[:, None])[:, 0]
+            assert O.rel_fro(t.matvec(x.copy()), want) < REL
+            assert O.rel_fro(t.matmat(np.asfortranarray(x[:, None]), "N")[:, 0], want) < REL
+            t.free()
+    finally:
+        lib.hodlr_b200_set_option(b"matvec_kernels", 1.0)
