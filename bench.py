@@ -706,7 +706,9 @@ def main():
                    "kind": "reference",
                    "sample": f"hmat_lib multiply_hodlr_dense k={k} on its own build at "
                              f"n={res['n']} (same kernel family; build {res['build_s']:.2f} s)",
-                   "build_s": res["build_s"], "cpu": res.get("cpu")}
+                   "build_s": res["build_s"], "cpu": res.get("cpu"),
+                   "matvec_n1024_us": res.get("matvec_n1024_us"),
+                   "hxh_n4096_s": res.get("hxh_n4096_s")}
         else:
             cpu = {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": "failed: " + res["error"]}

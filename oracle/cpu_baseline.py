@@ -31,6 +31,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--no-side", action="store_true",
+                    help="skip the n = 1024 H x and n = 4096 H x H timings")
     args = ap.parse_args()
 
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
@@ -62,12 +64,53 @@ def main():
     step = float(np.median(times))
     nbytes = 8.0 * storage + 16.0 * args.n * args.k
     flops = 2.0 * args.k * storage
-    print(json.dumps(dict(
+    out = dict(
         n=args.n, height=args.height, k=args.k, tol=args.tol, threads=args.threads,
         build_s=build_s, matmat_s=step, matmat_gbs=nbytes / step / 1e9,
         matmat_gflops=flops / step / 1e9, storage=int(storage),
         max_rank=int(max(td.ranks().values())),
-        cpu=_cpu_model())))
+        cpu=_cpu_model())
+    if not args.no_side:
+        out.update(side_workloads(args.threads))
+    print(json.dumps(out))
+
+
+def side_workloads(threads: int) -> dict:
+    """The reference on the two smaller workloads of the hot path: H x on the
+    n = 1024 Gaussian tree (the workload's own size), and H_A H_B on the
+    Gaussian / Matern-3/2 pair on sorted 1D points at n = 4096 (depth 5; the
+    n = 16384 pair takes the reference minutes to build)."""
+    import numpy as np
+
+    from hmat_lib_b200 import workloads as W
+    from oracle import ref_lib
+
+    res = {}
+    w = W.WORKLOADS["gauss1d_n1024"]
+    pts = W.workload_points("gauss1d_n1024")
+    a = W.kernel_matrix(pts, w["kind"], w["length"], w["diag"])
+    ref_lib.set_omp_threads(threads)
+    ref_lib.set_blas_threads(1)
+    t = ref_lib.build(a, w["height"], w["tol"])
+    ref_lib.set_blas_threads(threads)
+    x = np.random.default_rng(0).standard_normal(w["n"])
+    for _ in range(20):
+        ref_lib.multiply_vector(t, x)
+    reps = 200
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ref_lib.multiply_vector(t, x)
+    res["matvec_n1024_us"] = (time.perf_counter() - t0) / reps * 1e6
+    n = 4096
+    pts, ka, kb = W.hxh_pair(n, seed=3)
+    ref_lib.set_blas_threads(1)
+    ta = ref_lib.build(W.kernel_matrix(pts, *ka), 5, 1e-8)
+    tb = ref_lib.build(W.kernel_matrix(pts, *kb), 5, 1e-8)
+    ref_lib.set_blas_threads(threads)
+    t0 = time.perf_counter()
+    ref_lib.multiply_hodlr_hodlr(ta, tb, 1e-8)
+    res["hxh_n4096_s"] = time.perf_counter() - t0
+    return res
 
 
 def _cpu_model():
