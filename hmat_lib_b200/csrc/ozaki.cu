@@ -102,15 +102,31 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
     // then each copy 1/split of the A block and of the B block
     long long g = 0;   // K-blocks issued by this CTA
     bool stop = false;
+    // descriptors run one tile ahead: the next tile's OzTile is loaded when a
+    // tile starts and its segment descriptors (one per lane, nseg <= 32) after
+    // the tile's first K-block is issued, so no descriptor load stalls the
+    // ring at a tile or segment boundary
+    OzTile T{};
+    OzSeg Gl{};
+    if (tile_first < tile_end) {
+      T = tiles[tile_first];
+      if (lane < T.nseg) Gl = segs[T.seg0 + lane];
+    }
     for (int tile = tile_first; tile < tile_end && !stop; ++tile) {
       stop = __shfl_sync(0xffffffffu, (int)bad, 0) != 0;
       if (stop) break;
-      const OzTile T = tiles[tile];
+      const bool more = tile + 1 < tile_end;
+      OzTile Tn{};
+      if (more) Tn = tiles[tile + 1];
+      OzSeg Gn{};
+      bool next_segs = !more;
       const uint32_t bbytes = (uint32_t)oz_bblock(T.nw);
       const uint32_t ca = (uint32_t)kOzABlock / split, cb = bbytes / split;
-      for (int s = T.seg0; s < T.seg0 + T.nseg && !stop; ++s) {
-        const OzSeg G = segs[s];
-        for (int kb = 0; kb < G.nkb; ++kb) {
+      for (int q = 0; q < T.nseg && !stop; ++q) {
+        const uint8_t *ga = (const uint8_t *)__shfl_sync(0xffffffffu, (unsigned long long)Gl.a, q);
+        const uint8_t *gb = (const uint8_t *)__shfl_sync(0xffffffffu, (unsigned long long)Gl.b, q);
+        const int nkb = __shfl_sync(0xffffffffu, Gl.nkb, q);
+        for (int kb = 0; kb < nkb; ++kb) {
           const int st = (int)(g % kStages);
           const long long use = g / kStages;
           int ok = 1;
@@ -126,14 +142,21 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
           if (lane == 0) umma::mbar_expect_tx(&full[st], (uint32_t)kOzABlock + bbytes);
           __syncwarp();
           if (lane < split) {
-            umma::bulk_g2s(dst + lane * ca, G.a + (long long)kb * kOzABlock + lane * ca, ca,
+            umma::bulk_g2s(dst + lane * ca, ga + (long long)kb * kOzABlock + lane * ca, ca,
                            &full[st]);
-            umma::bulk_g2s(dst + kOzABlock + lane * cb, G.b + (long long)kb * bbytes + lane * cb,
+            umma::bulk_g2s(dst + kOzABlock + lane * cb, gb + (long long)kb * bbytes + lane * cb,
                            cb, &full[st]);
           }
           ++g;
+          if (!next_segs) {
+            if (lane < Tn.nseg) Gn = segs[Tn.seg0 + lane];
+            next_segs = true;
+          }
         }
       }
+      if (!next_segs && lane < Tn.nseg) Gn = segs[Tn.seg0 + lane];
+      T = Tn;
+      Gl = Gn;
     }
     // copies still in flight land before the CTA may exit
     if (lane == 0)
@@ -145,8 +168,11 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
       long long g = 0;
       int lt = 0;
       bool ok = true;
+      OzTile Tn{};
+      if (tile_first < tile_end) Tn = tiles[tile_first];
       for (int tile = tile_first; tile < tile_end && ok && !bad; ++tile, ++lt) {
-        const OzTile T = tiles[tile];
+        const OzTile T = Tn;
+        if (tile + 1 < tile_end) Tn = tiles[tile + 1];   // lands while this tile runs
         if (lt > 0 && !wait_or_abort(&tmem_empty, (uint32_t)((lt - 1) & 1), &bad)) {
           ok = false;
           break;
@@ -156,9 +182,8 @@ ozaki_gemm_kernel(const OzSeg *__restrict__ segs, const OzTile *__restrict__ til
         const int maxcnt = min(kOzSlices, 256 / nw);
         const uint32_t bslice = (uint32_t)nw * kOzKBlock;
         bool first = true;
-        for (int s = T.seg0; s < T.seg0 + T.nseg && ok; ++s) {
-          const int nkb = segs[s].nkb;
-          for (int kb = 0; kb < nkb; ++kb, ++g) {
+        {
+          for (int kb = 0; kb < T.nkb; ++kb, ++g) {
             const int st = (int)(g % kStages);
             if (!wait_or_abort(&full[st], (uint32_t)((g / kStages) & 1), &bad)) {
               ok = false;
@@ -540,8 +565,12 @@ std::vector<int> ozaki_schedule(std::vector<OzTile> &tiles, const std::vector<Oz
   constexpr long long kTileCost = 160;
   std::vector<long long> cost(tiles.size());
   for (size_t i = 0; i < tiles.size(); ++i) {
+    HB_REQUIRE(tiles[i].nseg >= 0 && tiles[i].nseg <= 32, INPUT_ERROR,
+               "int8 product: more than 32 segments in a tile");
     long long kb = 0;
     for (int q = tiles[i].seg0; q < tiles[i].seg0 + tiles[i].nseg; ++q) kb += segs[q].nkb;
+    HB_REQUIRE(kb < (1LL << 31), INPUT_ERROR, "int8 product: K range too long");
+    tiles[i].nkb = (int)kb;
     cost[i] = kb * tiles[i].nw + kTileCost;
   }
   std::vector<int> order(tiles.size());

@@ -62,7 +62,8 @@ struct OzSeg {
 // rmax, if set, receives (atomic max, double bits) the largest |result| of
 // every row of the tile.
 struct OzTile {
-  int seg0, nseg;
+  int seg0, nseg;  // at most 32 segments
+  int nkb;         // K-blocks of all segments (set by ozaki_schedule)
   int rows, cols;
   int nw;          // B tile width: multiple of 16, <= 64
   int atomic;      // 1: add atomically (K split over several tiles)
