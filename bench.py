@@ -160,9 +160,10 @@ def int8_peak_tops(torch, dev):
         return 2.0 * bf16, "2 x measured BF16 dense peak (int8 GEMM unavailable)"
 
 
-def run_cpu_baseline(n: int, k: int):
+def run_cpu_baseline(n: int, k: int, steps: int = 3, warmup: int = 1):
     cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--n", str(n),
-           "--height", str(max(1, (n // 128).bit_length() - 1)), "--k", str(k), "--steps", "3"]
+           "--height", str(max(1, (n // 128).bit_length() - 1)), "--k", str(k),
+           "--steps", str(steps), "--warmup", str(warmup)]
     try:
         out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
         line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
@@ -382,7 +383,10 @@ def reference_arm(args, rank):
     oracle/_ref) on this box's host cores, same metric and unit."""
     if rank != 0:
         return
-    res = run_cpu_baseline(args.cpu_n, 256)
+    # every step is one multiply_hodlr_dense of the bounded sample (n = 4096,
+    # about 25 ms on 8 cores), so K steps stay within seconds to minutes
+    steps, warmup = max(1, args.steps), max(0, args.warmup)
+    res = run_cpu_baseline(args.cpu_n, 256, steps, warmup)
     if "error" in res:
         print(json.dumps({"impl": "reference", "unavailable": res["error"]}))
         return
@@ -393,7 +397,8 @@ def reference_arm(args, rank):
     value = res["matmat_gbs"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s",
-        "n_gpus": args.gpus, "steps": 3, "warmup": 1, "ms_per_step": res["matmat_s"] * 1e3,
+        "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+        "ms_per_step": res["matmat_s"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": {"workload": WORKLOAD, "n": res["n"],
                                         "height": res["height"], "k": 256, "tol": 1e-8},
@@ -401,6 +406,7 @@ def reference_arm(args, rank):
         "build_s_extrapolated_n32768": res["build_s"] * (32768 / res["n"]) ** 3,
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": nthreads,
                          "kind": "reference", "sample": sample, "cpu": res.get("cpu")},
+        "matvec_n1024_us": res.get("matvec_n1024_us"), "hxh_n4096_s": res.get("hxh_n4096_s"),
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
