@@ -250,7 +250,9 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   for (int b = 0; b < nb; ++b)
     if (g.blocks[b].s) work += (long long)st.ntn[b] * st.nw[b] * (g.blocks[b].n / kOzKBlock);
   work *= nja;
-  const long long target = std::max<long long>(work / (3LL * num_sms()), 64LL * 16);
+  // about `per_cta` tiles' worth of work per CTA (option ozaki_phase1_tiles_per_cta)
+  const long long per_cta = std::max(1LL, (long long)option("ozaki_phase1_tiles_per_cta", 2.0));
+  const long long target = std::max<long long>(work / (per_cta * num_sms()), 64LL * 16);
   std::vector<int> nch(nb, 1);
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
