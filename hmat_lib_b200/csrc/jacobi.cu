@@ -57,6 +57,32 @@ __device__ __forceinline__ void team_sync() {
     __syncthreads();
 }
 
+// (x, y) <- (c x - s y, s x + c y) over `len` elements, the warp's lanes
+// striding by 32, four elements per lane in flight.
+template <bool kTeam>
+__device__ __forceinline__ void rotate_pair(double *xp, double *yp, int len, int lane, double cs,
+                                            double sn) {
+  int i0 = lane;
+  for (; i0 + 96 < len; i0 += 128) {
+    double x[4], y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x[u] = gld<kTeam>(xp + i0 + 32 * u);
+      y[u] = gld<kTeam>(yp + i0 + 32 * u);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      gst<kTeam>(xp + i0 + 32 * u, cs * x[u] - sn * y[u]);
+      gst<kTeam>(yp + i0 + 32 * u, sn * x[u] + cs * y[u]);
+    }
+  }
+  for (int i = i0; i < len; i += 32) {
+    const double x = gld<kTeam>(xp + i), y = gld<kTeam>(yp + i);
+    gst<kTeam>(xp + i, cs * x - sn * y);
+    gst<kTeam>(yp + i, sn * x + cs * y);
+  }
+}
+
 // One problem, by one CTA (kTeam false) or by the kJCluster CTAs of a
 // cluster (kTeam true, `crank` = this CTA's rank in it): the disjoint pairs
 // of a round are spread over every warp of the team, rounds are separated by
@@ -77,6 +103,7 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
 
   double *G = P.G, *W = P.W;
   const int gtid = crank * blockDim.x + tid, gthreads = team * blockDim.x;
+  double fro2 = 0.0;   // this thread's share of ||A||_F^2
   for (long long e = gtid; e < (long long)R * C; e += gthreads) {
     const int r = (int)(e % R), c = (int)(e / R);
     // logical element (i, j) of the m x n input
@@ -87,11 +114,41 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
                    : kernel_entry(gen, P.gen_r0 + i, P.gen_c0 + j);
     else
       a = P.transA ? P.A[j + (long long)i * P.lda] : P.A[i + (long long)j * P.lda];
+    fro2 = fma(a, a, fro2);
     gst<kTeam>(G + e, a);
   }
   for (long long e = gtid; e < (long long)C * C; e += gthreads)
     gst<kTeam>(W + e, ((e % C) == (e / C)) ? 1.0 : 0.0);
   team_sync<kTeam>();
+
+  // ||A||_F over the team
+  fro2 = warp_sum(fro2);
+  if (lane == 0) s_off[warp] = fro2;
+  __syncthreads();
+  double f2 = 0.0;
+  for (int w = 0; w < nwarps; ++w) f2 += s_off[w];
+  if constexpr (kTeam) {
+    cg::cluster_group cl = cg::this_cluster();
+    if (tid == 0) s_team_off = f2;
+    cl.sync();
+    f2 = 0.0;
+    for (int rk = 0; rk < team; ++rk) f2 += *cl.map_shared_rank(&s_team_off, rk);
+    cl.sync();
+  }
+  __syncthreads();
+  // Pairs with a column of norm below theta are neither rotated nor tested:
+  // all such columns together hold at most sqrt(C) theta = 1e-3 tol s_0 of the
+  // matrix (||A||_F / C <= s_0 / sqrt(C) for the relative rule), so no
+  // singular value moves by more than 0.1% of the truncation threshold
+  // (Weyl) and none of theirs reaches it.  Columns at rounding level otherwise
+  // keep the sweeps going: their computed cosines with any column are
+  // rounding noise.  No skipping when every singular value is kept.
+  double theta = 0.0;
+  if (prm.trunc == Truncation::Relative)
+    theta = 1e-3 * prm.tol * sqrt(f2) / C;
+  else if (prm.trunc == Truncation::Absolute)
+    theta = 1e-3 * prm.tol / sqrt((double)C);
+  const double skip2 = theta * theta;
 
   // a computed dot product of length R carries ~sqrt(R) eps relative noise:
   // below that no rotation can make progress
@@ -115,8 +172,25 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
         if (a >= C || b >= C) continue;
         const int p = min(a, b), q = max(a, b);
         double *gp = G + (long long)p * R, *gq = G + (long long)q * R;
+        // four elements per lane in flight (each sum keeps the element order
+        // of a plain loop, so the arithmetic is unchanged)
         double al = 0.0, be = 0.0, ga = 0.0;
-        for (int i = lane; i < R; i += 32) {
+        int i0 = lane;
+        for (; i0 + 96 < R; i0 += 128) {
+          double x[4], y[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            x[u] = gld<kTeam>(gp + i0 + 32 * u);
+            y[u] = gld<kTeam>(gq + i0 + 32 * u);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            al = fma(x[u], x[u], al);
+            be = fma(y[u], y[u], be);
+            ga = fma(x[u], y[u], ga);
+          }
+        }
+        for (int i = i0; i < R; i += 32) {
           const double x = gld<kTeam>(gp + i), y = gld<kTeam>(gq + i);
           al = fma(x, x, al);
           be = fma(y, y, be);
@@ -126,6 +200,7 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
         be = warp_sum(be);
         ga = warp_sum(ga);
         if (ga == 0.0 || al <= 0.0 || be <= 0.0) continue;
+        if (al <= skip2 || be <= skip2) continue;
         const double rel = fabs(ga) / (sqrt(al) * sqrt(be));
         off = fmax(off, rel);
         if (rel <= conv) continue;
@@ -136,17 +211,8 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
                              ? 0.5 / zeta
                              : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
         const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-        for (int i = lane; i < R; i += 32) {
-          const double x = gld<kTeam>(gp + i), y = gld<kTeam>(gq + i);
-          gst<kTeam>(gp + i, cs * x - sn * y);
-          gst<kTeam>(gq + i, sn * x + cs * y);
-        }
-        double *wp = W + (long long)p * C, *wq = W + (long long)q * C;
-        for (int i = lane; i < C; i += 32) {
-          const double x = gld<kTeam>(wp + i), y = gld<kTeam>(wq + i);
-          gst<kTeam>(wp + i, cs * x - sn * y);
-          gst<kTeam>(wq + i, sn * x + cs * y);
-        }
+        rotate_pair<kTeam>(gp, gq, R, lane, cs, sn);
+        rotate_pair<kTeam>(W + (long long)p * C, W + (long long)q * C, C, lane, cs, sn);
       }
       team_sync<kTeam>();
     }

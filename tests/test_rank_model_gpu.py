@@ -181,7 +181,11 @@ def test_fallback_when_prediction_is_too_low(trained):
         tl, sl, fl = _build(a, n, h, True, length)
         assert sl["fallbacks"] == np.sum(fl[:, 11] > 0) > 0
         assert np.max(np.abs(tp.ranks() - tl.ranks())) <= 1
-        assert _error_vs_dense(a, tl, n) <= 1.25 * _error_vs_dense(a, tp, n) + 1e-12
+        # a rank one lower at the threshold (or another sketch basis) moves the
+        # error by tens of percent at the tolerance's scale; the sketch
+        # products add split-K partial sums in a run-dependent order, so the
+        # bound is the one of the matching-build test above
+        assert _error_vs_dense(a, tl, n) <= 1.5 * _error_vs_dense(a, tp, n) + 1e-12
         tp.free()
         tl.free()
     finally:
