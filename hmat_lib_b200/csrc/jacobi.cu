@@ -25,6 +25,7 @@ namespace {
 
 constexpr int kJThreads = 256;
 constexpr int kJCluster = 8;        // CTAs per problem cluster
+constexpr int kJUnroll = 8;         // column elements per lane in flight in the pair loops
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -58,28 +59,26 @@ __device__ __forceinline__ void team_sync() {
 }
 
 // (x, y) <- (c x - s y, s x + c y) over `len` elements, the warp's lanes
-// striding by 32, four elements per lane in flight.
+// striding by 32, eight elements per lane in flight.
 template <bool kTeam>
 __device__ __forceinline__ void rotate_pair(double *xp, double *yp, int len, int lane, double cs,
                                             double sn) {
-  int i0 = lane;
-  for (; i0 + 96 < len; i0 += 128) {
-    double x[4], y[4];
+  for (int i0 = lane; i0 < len; i0 += 32 * kJUnroll) {
+    double x[kJUnroll], y[kJUnroll];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      x[u] = gld<kTeam>(xp + i0 + 32 * u);
-      y[u] = gld<kTeam>(yp + i0 + 32 * u);
+    for (int u = 0; u < kJUnroll; ++u) {
+      const int i = i0 + 32 * u;
+      x[u] = i < len ? gld<kTeam>(xp + i) : 0.0;
+      y[u] = i < len ? gld<kTeam>(yp + i) : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      gst<kTeam>(xp + i0 + 32 * u, cs * x[u] - sn * y[u]);
-      gst<kTeam>(yp + i0 + 32 * u, sn * x[u] + cs * y[u]);
+    for (int u = 0; u < kJUnroll; ++u) {
+      const int i = i0 + 32 * u;
+      if (i < len) {
+        gst<kTeam>(xp + i, cs * x[u] - sn * y[u]);
+        gst<kTeam>(yp + i, sn * x[u] + cs * y[u]);
+      }
     }
-  }
-  for (int i = i0; i < len; i += 32) {
-    const double x = gld<kTeam>(xp + i), y = gld<kTeam>(yp + i);
-    gst<kTeam>(xp + i, cs * x - sn * y);
-    gst<kTeam>(yp + i, sn * x + cs * y);
   }
 }
 
@@ -172,29 +171,24 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
         if (a >= C || b >= C) continue;
         const int p = min(a, b), q = max(a, b);
         double *gp = G + (long long)p * R, *gq = G + (long long)q * R;
-        // four elements per lane in flight (each sum keeps the element order
-        // of a plain loop, so the arithmetic is unchanged)
+        // eight elements per lane in flight, the last chunk predicated (each
+        // sum keeps the element order of a plain loop: arithmetic unchanged)
         double al = 0.0, be = 0.0, ga = 0.0;
-        int i0 = lane;
-        for (; i0 + 96 < R; i0 += 128) {
-          double x[4], y[4];
+        for (int i0 = lane; i0 < R; i0 += 32 * kJUnroll) {
+          double x[kJUnroll], y[kJUnroll];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            x[u] = gld<kTeam>(gp + i0 + 32 * u);
-            y[u] = gld<kTeam>(gq + i0 + 32 * u);
+          for (int u = 0; u < kJUnroll; ++u) {
+            const int i = i0 + 32 * u;
+            x[u] = i < R ? gld<kTeam>(gp + i) : 0.0;
+            y[u] = i < R ? gld<kTeam>(gq + i) : 0.0;
           }
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            al = fma(x[u], x[u], al);
-            be = fma(y[u], y[u], be);
-            ga = fma(x[u], y[u], ga);
-          }
-        }
-        for (int i = i0; i < R; i += 32) {
-          const double x = gld<kTeam>(gp + i), y = gld<kTeam>(gq + i);
-          al = fma(x, x, al);
-          be = fma(y, y, be);
-          ga = fma(x, y, ga);
+          for (int u = 0; u < kJUnroll; ++u)
+            if (i0 + 32 * u < R) {
+              al = fma(x[u], x[u], al);
+              be = fma(y[u], y[u], be);
+              ga = fma(x[u], y[u], ga);
+            }
         }
         al = warp_sum(al);
         be = warp_sum(be);
