@@ -102,14 +102,24 @@ std::unique_ptr<DeviceTree> dtree_create(const Geometry &g_in, cudaStream_t stre
     off += align_up((long long)b.n * b.s);
   }
   t->arena_elems = off;
-  HB_CUDA(cudaMalloc(&t->arena, std::max<long long>(off, 1) * sizeof(double)));
-  HB_CUDA(cudaMalloc(&t->d_leaves, std::max<size_t>(t->leaves.size(), 1) * sizeof(LeafDesc)));
-  HB_CUDA(cudaMalloc(&t->d_blocks, std::max<size_t>(g.blocks.size(), 1) * sizeof(BlockDesc)));
+  // from the device's stream-ordered pool (kept mapped, see keep_pool_memory):
+  // a build allocates its tree while the GPU waits, and a synchronous
+  // cudaMalloc of the arena had to map fresh pages there.  cudaFree releases
+  // these allocations like any other.
+  keep_pool_memory();
+  HB_CUDA(cudaMallocAsync((void **)&t->arena, std::max<long long>(off, 1) * sizeof(double),
+                          stream));
+  HB_CUDA(cudaMallocAsync((void **)&t->d_leaves,
+                          std::max<size_t>(t->leaves.size(), 1) * sizeof(LeafDesc), stream));
+  HB_CUDA(cudaMallocAsync((void **)&t->d_blocks,
+                          std::max<size_t>(g.blocks.size(), 1) * sizeof(BlockDesc), stream));
   HB_CUDA(cudaMemcpyAsync(t->d_leaves, t->leaves.data(), t->leaves.size() * sizeof(LeafDesc),
                           cudaMemcpyHostToDevice, stream));
   if (!g.blocks.empty())
     HB_CUDA(cudaMemcpyAsync(t->d_blocks, g.blocks.data(), g.blocks.size() * sizeof(BlockDesc),
                             cudaMemcpyHostToDevice, stream));
+  // the allocations (stream-ordered on `stream`) and descriptors are ready
+  // for use on any stream once this returns
   HB_CUDA(cudaStreamSynchronize(stream));
   return t;
 }
