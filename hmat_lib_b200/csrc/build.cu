@@ -619,7 +619,10 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   // training data): the fewest leading singular values whose discarded tail
   // has Frobenius norm <= tol * s_0
   std::vector<int> fro_rank(sk.size(), 0);
-  std::vector<std::vector<double>> core_sig(record ? sk.size() : 0);
+  // (training data only: the singular values of every core come back to the
+  // host, so a learned build without option record_features skips it)
+  const bool want_fro = option("record_features", 0.0) != 0.0;
+  std::vector<std::vector<double>> core_sig(want_fro ? sk.size() : 0);
   for (size_t i = 0; i < core_sig.size(); ++i) {
     core_sig[i].resize(sk[i].ell);
     HB_CUDA(cudaMemcpyAsync(core_sig[i].data(), sprobs[i].sigma, sizeof(double) * sk[i].ell,

@@ -223,8 +223,9 @@ int hodlr_b200_rank_model_adam(float *params, const float *grad, float *m, float
  * final rank, the predicted rank (-1 without a model), the first sketch
  * width, whether the block fell back to adaptive growth, the final sketch
  * width, the Frobenius epsilon-rank (fewest leading singular values whose
- * discarded tail has Frobenius norm <= tol * s_0).  Rows of 14 floats;
- * returns the number of rows. */
+ * discarded tail has Frobenius norm <= tol * s_0; computed only with option
+ * "record_features", 0 otherwise).  Rows of 14 floats; returns the number of
+ * rows. */
 int hodlr_b200_build_features(float *out, int capacity_rows);
 
 #ifdef __cplusplus
