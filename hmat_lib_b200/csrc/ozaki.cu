@@ -6,7 +6,8 @@
 //   warp 0               producer: per K-block the A block (all S slices of
 //                        128 lines) and the B block, each as 1-8 bulk copies
 //                        issued by as many lanes, into a six-stage ring,
-//                        completion on full[stage];
+//                        completion on full[stage]; the next tile's
+//                        descriptors are fetched while a tile streams;
 //   warp 1 (one thread)  MMA issuer: per K-block the S(S+1)/2 slice products
 //                        as 8 MMAs (slice p of A against slices q = 1 .. S+1-p
 //                        of B, which sit next to each other in shared memory,
@@ -16,11 +17,13 @@
 //                        to tmem_full;
 //   warps 2-9            epilogue (two warps per quarter of the TMEM lanes,
 //                        alternate 16-column chunks): wait tmem_full, read the
-//                        S int32 groups of their 32 lanes, recombine in FP64,
-//                        release the accumulators (tmem_empty), then scale by
+//                        S int32 groups of their 32 lanes, combine them (each
+//                        triple exactly in 64-bit integers, the two triples
+//                        in FP64), release the accumulators (tmem_empty),
+//                        then scale by
 //                        2^(e_r + f_j) and store or atomically add the tile
 //                        while the next tile's MMAs run.
-// The warp also owns the TMEM allocation (512 columns: S groups of <= 64).
+// Warp 1 also owns the TMEM allocation (512 columns: S groups of <= 64).
 // Every barrier wait is bounded; a wait that runs out sets the CTA's abort
 // flag, every role leaves its loop, the producer waits (bounded) for its
 // copies in flight, the MMA thread for its MMAs, and the kernel reports
