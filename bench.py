@@ -88,6 +88,13 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, timeout: float = 5.0):
+        """Blocks until the sampler has printed its first line (nvidia-smi
+        takes a moment to start) or `timeout` seconds pass."""
+        t0 = time.perf_counter()
+        while self.proc and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.02)
+
     def __exit__(self, *exc):
         if self.proc:
             self.proc.terminate()
@@ -553,8 +560,19 @@ def main():
         lib.hodlr_b200_set_option(b"record_phase_times", 1.0)
         lib.hodlr_b200_phase_times(None, 0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        launches0 = lib.hodlr_b200_kernel_launches()
         with ClockSampler(local) as clk:
+            # The timed region can be shorter than the sampler's 200 ms
+            # interval, so the clocks are sampled over a run of the same
+            # product of at least one second right before it, and during it.
+            clk.wait_first()
+            t_pre = time.perf_counter()
+            while time.perf_counter() - t_pre < 1.0:
+                for _ in range(10):
+                    tree.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh,
+                                precision=precision)
+                stream.synchronize()
+            lib.hodlr_b200_phase_times(None, 0)
+            launches0 = lib.hodlr_b200_kernel_launches()
             torch.cuda.nvtx.range_push(tag)     # lets ncu select the timed launches
             e0.record(stream)
             for _ in range(steps):
@@ -573,7 +591,10 @@ def main():
             ms_total = t.item()
             pg.barrier()
         torch.cuda.synchronize()
-        return dict(ms=ms_total / steps, launches=int(launches), clocks=clk.summary(),
+        clocks = clk.summary()
+        clocks["window"] = ("nvidia-smi every 200 ms over >= 1 s of the same product run "
+                            "immediately before the timed region, and during it")
+        return dict(ms=ms_total / steps, launches=int(launches), clocks=clocks,
                     p1=pt[0] / max(pt[2], 1), p2=pt[1] / max(pt[2], 1),
                     k1=pt[3] / max(pt[2], 1), k2=pt[4] / max(pt[2], 1))
 
@@ -685,7 +706,9 @@ def main():
         op2 += 6.0 * nb * _cdiv(s_b, 32) * 32 + 6.0 * _cdiv(s_b, 32) * 32 * _cdiv(k, 64) * 64
     int8_bytes = {"phase1": op1, "phase2": op2}
     # DRAM bytes (read + write) per launch / int8 operand bytes, measured by
-    # ncu on the n = 16384 instance (profiles/matmat_mixed_int8_n32768_k256.md)
+    # ncu on the n = 16384 instance of this workload family (a capture of the
+    # n = 32768 launch does not fit the profiler's size limit); applied to
+    # the operand bytes at this n
     traffic_ratio_i8 = {"phase1": 0.89, "phase2": 0.90}
     peak_i8, peak_src = int8_peak_tops(torch, dev)
     peak64 = fp64_peak_tflops(torch, dev)
@@ -701,7 +724,7 @@ def main():
     dom64_ms = r64["p1"] if dom64 == "phase1" else r64["p2"]
     achieved64 = 2.0 * k * el[dom64] / (dom64_ms * 1e-3) / 1e12
     # DRAM traffic / algorithmic bytes of the FP64 phases, measured by ncu on
-    # the n = 16384 instance (profiles/matmat_fp64_gemm_n16384_k256.md)
+    # the n = 16384 instance of this workload family
     traffic_ratio64 = {"phase1": 1.31, "phase2": 1.14}
     bytes64 = {"phase1": 8.0 * sn + 8.0 * n * k, "phase2": 8.0 * (leaves_el + sn) + 16.0 * n * k}
     cpu = None
@@ -755,6 +778,8 @@ def main():
                      "achieved_incl_slicing": achieved_phase,
                      "frac_incl_slicing": achieved_phase / peak_i8,
                      "traffic": traffic_ratio_i8[dom] * int8_bytes[dom],
+                     "traffic_source": "ncu DRAM bytes / operand bytes of this kernel at "
+                                       "n = 16384, times the operand bytes at this n",
                      "int8_operand_bytes": int8_bytes[dom],
                      "int8_operand_bytes_by_phase": int8_bytes,
                      "peak_source": peak_src,
@@ -767,6 +792,8 @@ def main():
                               "achieved": achieved64, "peak": peak64, "unit": "TFLOP/s",
                               "frac": achieved64 / peak64,
                               "traffic": traffic_ratio64[dom64] * bytes64[dom64],
+                              "traffic_source": "ncu DRAM bytes / algorithmic bytes at "
+                                                "n = 16384, times the bytes at this n",
                               "algorithmic_bytes": bytes64[dom64],
                               "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                               "phase_ms": {"phase1": r64["p1"], "phase2": r64["p2"]}},

@@ -20,6 +20,9 @@ SVD_FAILURE = 2
 SVD_ALLOCATION_FAILURE = 3
 INPUT_ERROR = 4
 QR_FAILURE = 5
+# libhodlr_b200's own status for a failed CUDA call or launch
+# (include/hmat_lib/hodlr_b200.h)
+HODLR_B200_CUDA_ERROR = 100
 
 ERROR_NAMES = {
     SUCCESS: "SUCCESS",
@@ -28,6 +31,7 @@ ERROR_NAMES = {
     SVD_ALLOCATION_FAILURE: "SVD_ALLOCATION_FAILURE",
     INPUT_ERROR: "INPUT_ERROR",
     QR_FAILURE: "QR_FAILURE",
+    HODLR_B200_CUDA_ERROR: "HODLR_B200_CUDA_ERROR",
 }
 
 DP = C.POINTER(C.c_double)
@@ -127,6 +131,8 @@ B200_API = {
     "hodlr_b200_matmat_dev": (
         C.c_int, [VP, C.c_int, C.c_int, VP, C.c_int, C.c_int, VP, C.c_int, VP]),
     "hodlr_b200_hxh_dev": (C.c_int, [VP, VP, C.c_double, C.POINTER(VP), IP]),
+    "hodlr_b200_recompress_dev": (C.c_int, [C.c_int, C.c_int, C.c_int, VP, C.c_int, VP, C.c_int,
+                                            C.c_double, C.c_int, VP, VP, IP, VP]),
     "hodlr_b200_sync_tree": (C.c_int, [TP]),
     "hodlr_b200_kernel_launches": (C.c_longlong, []),
     "hodlr_b200_set_option": (C.c_int, [C.c_char_p, C.c_double]),
@@ -202,6 +208,22 @@ def load(required: bool = True):
     _declare(lib, B200_API)
     _LIB = lib
     return lib
+
+
+def built_source_hash(lib) -> str:
+    """Digest of the sources the loaded library was built from (the last word
+    of hodlr_b200_version())."""
+    return lib.hodlr_b200_version().decode().rsplit(" ", 1)[-1]
+
+
+def check_source_hash(lib) -> None:
+    """Raises if the loaded library was not built from the sources beside
+    it (rebuild with `python -m hmat_lib_b200.build`)."""
+    from . import build
+    want, got = build.source_hash(), built_source_hash(lib)
+    if want != got:
+        raise RuntimeError(f"{LIB_NAME} was built from other sources (library {got}, "
+                           f"sources {want}); rebuild with `python -m hmat_lib_b200.build`")
 
 
 def load_hmat_abi(path: str):

@@ -9,6 +9,7 @@ travels with the source tree.
 from __future__ import annotations
 
 import glob
+import hashlib
 import os
 import subprocess
 import sys
@@ -28,6 +29,35 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE
 
 def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+
+
+def source_hash() -> str:
+    """SHA-256 (first 16 hex digits) of every source and header the library
+    is built from (csrc/ and include/hmat_lib/, paths and contents, sorted).
+    Compiled into the library and returned by hodlr_b200_version(), so a
+    caller can tell whether a binary was built from the sources beside it."""
+    files = sorted(_sources() + glob.glob(os.path.join(CSRC, "*.h")) +
+                   glob.glob(os.path.join(CSRC, "*.cuh")) +
+                   glob.glob(os.path.join(INCLUDE, "hmat_lib", "*.h")))
+    h = hashlib.sha256()
+    for f in files:
+        h.update(os.path.relpath(f, os.path.dirname(HERE)).encode())
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def _hash_object(force: bool):
+    """Object file defining hb_source_hash() for the current sources."""
+    digest = source_hash()
+    src = os.path.join(BUILD, "source_hash.cpp")
+    text = ('// generated by hmat_lib_b200/build.py\n'
+            f'extern "C" const char *hb_source_hash(void) {{ return "{digest}"; }}\n')
+    old = open(src).read() if os.path.exists(src) else None
+    if old != text:
+        with open(src, "w") as f:
+            f.write(text)
+    return _compile(src, force, 0.0)
 
 
 def _newest_header():
@@ -57,6 +87,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     srcs = _sources()
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         results = list(ex.map(lambda s: _compile(s, force, hdr), srcs))
+    results.append(_hash_object(force))
     errs = [e for _, e in results if e]
     if errs:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errs))

@@ -191,6 +191,8 @@ std::shared_ptr<DeviceTree> subtree_device(const HODLRInternalNode *internal, in
 
 }  // namespace
 
+extern "C" const char *hb_source_hash(void);
+
 extern "C" {
 
 // ------------------------------------------------------------ construction
@@ -401,7 +403,12 @@ int multiply_hodlr_hodlr(const TreeHODLR *hodlr1, const TreeHODLR *hodlr2, TreeH
 
 // ------------------------------------------------------------ extensions
 
-const char *hodlr_b200_version(void) { return "hodlr-b200 0.1 (sm_100a)"; }
+const char *hodlr_b200_version(void) {
+  // hb_source_hash(): digest of the sources this binary was built from,
+  // generated at build time (hmat_lib_b200/build.py)
+  static const std::string v = std::string("hodlr-b200 0.2 (sm_100a) sources ") + hb_source_hash();
+  return v.c_str();
+}
 const char *hodlr_b200_last_error(void) { return last_error(); }
 long long hodlr_b200_kernel_launches(void) { return launches(); }
 
@@ -602,6 +609,18 @@ int hodlr_b200_hxh_dev(hodlr_b200_tree a, hodlr_b200_tree b, double svd_threshol
     return status;
   } catch (const Error &e) {
     return fail(ierr, e);
+  }
+}
+
+int hodlr_b200_recompress_dev(int m, int n, int s, const double *d_u, int ldu, const double *d_v,
+                              int ldv, double svd_threshold, int dense, double *d_u_out,
+                              double *d_v_out, int *rank, void *stream) {
+  if (!rank) return INPUT_ERROR;
+  try {
+    return recompress_one(m, n, s, d_u, ldu, d_v, ldv, svd_threshold, dense != 0, d_u_out,
+                          d_v_out, rank, as_stream(stream));
+  } catch (const Error &e) {
+    return fail(nullptr, e);
   }
 }
 

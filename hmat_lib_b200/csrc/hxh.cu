@@ -104,6 +104,166 @@ void block_qr(const std::vector<BlockQr> &probs, double *base, cudaStream_t s) {
   }
 }
 
+// ---- recompression of concatenated factors --------------------------------------
+// hmat_lib recompress (src/hodlr_algebra.c:97-211) and recompress_large_s
+// (:280-343), batched over blocks: blocked Householder QR of U and of V, SVD
+// of R_U R_V^T by Jacobi, absolute truncation (:160-163), U' = Q_U W Sigma,
+// V' = Q_V Z; a job marked dense decomposes U V^T itself instead.
+struct RecompJob {
+  int m = 0, n = 0, S = 0;   // block rows, columns, concatenated rank
+  long long u = 0, v = 0;    // workspace offsets of U (m x S, ld m) and V (n x S, ld n)
+  bool dense = false;        // SVD of the dense m x n product (recompress_large_s)
+  long long ru = 0, rv = 0, mm = 0, cs = 0, jws = 0, jo_u = 0, jo_v = 0, jsig = 0, dmat = 0;
+  bool active() const { return std::min(m, n) > 0 && S > 0; }
+};
+
+// Workspace of every job (`take(e)` returns the offset of e doubles);
+// returns the widest Jacobi problem.
+template <class Take>
+int recomp_layout(std::vector<RecompJob> &jobs, Take take) {
+  int max_c = 1;
+  for (RecompJob &j : jobs) {
+    const int mn = std::min(j.m, j.n);
+    if (mn == 0) continue;
+    const int Sb = std::max(j.S, 1);
+    if (j.dense) {
+      j.dmat = take((long long)j.m * j.n);
+      j.jws = take(jacobi_workspace(j.m, j.n));
+      j.jo_u = take((long long)j.m * mn);
+      j.jo_v = take((long long)j.n * mn);
+      j.jsig = take(mn);
+      max_c = std::max(max_c, mn);
+    } else {
+      j.ru = take((long long)Sb * Sb);
+      j.rv = take((long long)Sb * Sb);
+      j.mm = take((long long)Sb * Sb);
+      j.cs = take((long long)Sb * kPanel);
+      j.jws = take(jacobi_workspace(Sb, Sb));
+      j.jo_u = take((long long)Sb * Sb);
+      j.jo_v = take((long long)Sb * Sb);
+      j.jsig = take(Sb);
+      max_c = std::max(max_c, Sb);
+    }
+  }
+  return max_c;
+}
+
+// Runs the QRs, the dense products and the Jacobi SVDs of every job (the R
+// blocks of the workspace must be zero); returns each job's rank (0 for
+// inactive jobs) and the Jacobi status in *status.  Synchronises.
+std::vector<int> recomp_run(const std::vector<RecompJob> &jobs, double *work, double tol,
+                            int max_c, cudaStream_t s, int *status) {
+  GemmBases gb{};
+  for (int i = 0; i < kGemmBases; ++i) gb.p[i] = work;
+  const int nj = (int)jobs.size();
+  std::vector<BlockQr> qr_u, qr_v;
+  GemmBatch gd;   // dense products U V^T of the dense jobs
+  for (const RecompJob &j : jobs) {
+    if (!j.active()) continue;
+    if (j.dense) {
+      int p = gd.add(kWork, j.dmat, j.m, j.m, j.n);
+      gd.seg(p, kWork, j.u, j.m, 0, kWork, j.v, j.n, 1, j.S);
+    } else {
+      // the two QRs of a job share its C scratch: U's and V's run separately
+      qr_u.push_back(BlockQr{work + j.u, j.m, j.m, j.S, work + j.ru, j.S, work + j.cs});
+      qr_v.push_back(BlockQr{work + j.v, j.n, j.n, j.S, work + j.rv, j.S, work + j.cs});
+    }
+  }
+  gemm_f64_run(gd, gb, TileShape::M128N64, s);
+  block_qr(qr_u, work, s);
+  block_qr(qr_v, work, s);
+  {
+    GemmBatch gm;   // M = R_U R_V^T
+    for (const RecompJob &j : jobs) {
+      if (!j.active() || j.dense) continue;
+      int p = gm.add(kWork, j.mm, j.S, j.S, j.S);
+      gm.seg(p, kWork, j.ru, j.S, 0, kWork, j.rv, j.S, 1, j.S);
+    }
+    gemm_f64_run(gm, gb, TileShape::M64N128, s);
+  }
+  std::vector<JacobiProb> jp;
+  int *d_int = nullptr;
+  HB_CUDA(cudaMallocAsync((void **)&d_int, sizeof(int) * (nj + 1), s));
+  HB_CUDA(cudaMemsetAsync(d_int, 0, sizeof(int) * (nj + 1), s));
+  for (int i = 0; i < nj; ++i) {
+    const RecompJob &j = jobs[i];
+    if (!j.active()) continue;
+    JacobiProb p{};
+    p.transA = 0;
+    if (j.dense) {
+      p.A = work + j.dmat;
+      p.lda = j.m;
+      p.m = j.m;
+      p.n = j.n;
+      p.ldu = j.m;
+      p.ldv = j.n;
+    } else {
+      p.A = work + j.mm;
+      p.lda = j.S;
+      p.m = j.S;
+      p.n = j.S;
+      p.ldu = j.S;
+      p.ldv = j.S;
+    }
+    const long long R = std::max(p.m, p.n), C = std::min(p.m, p.n);
+    p.G = work + j.jws;
+    p.W = p.G + align_up(R * C);
+    p.U = work + j.jo_u;
+    p.V = work + j.jo_v;
+    p.sigma = work + j.jsig;
+    p.rank = d_int + i;
+    p.sweeps = nullptr;
+    jp.push_back(p);
+  }
+  if (!jp.empty()) {
+    JacobiParams prm;
+    prm.tol = tol;
+    prm.trunc = Truncation::Absolute;
+    prm.scale_u = 1;
+    prm.max_sweeps = (int)option("jacobi_max_sweeps", 60);
+    JacobiProb *d_jp = upload_vec(jp, s);
+    jacobi_svd_batched(d_jp, (int)jp.size(), prm, d_int + nj, max_c, s);
+    cudaFreeAsync(d_jp, s);
+  }
+  std::vector<int> ints(nj + 1, 0);
+  HB_CUDA(cudaMemcpyAsync(ints.data(), d_int, sizeof(int) * (nj + 1), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  dev_free(d_int, s);
+  *status = ints[nj];
+  ints.resize(nj);
+  for (int i = 0; i < nj; ++i)
+    if (!jobs[i].active()) ints[i] = 0;
+  return ints;
+}
+
+// Writes job i's recompressed factors, U' (m x r, ld m) at out + uo[i] and
+// V' (n x r, ld n) at out + vo[i], r = ranks[i].
+void recomp_finish(const std::vector<RecompJob> &jobs, const std::vector<int> &ranks,
+                   double *work, double *out, const std::vector<long long> &uo,
+                   const std::vector<long long> &vo, cudaStream_t s) {
+  GemmBases gb{};
+  for (int i = 0; i < kGemmBases; ++i) gb.p[i] = work;
+  gb.p[kOut] = out;
+  std::vector<CopyDesc> cp;
+  GemmBatch gf;
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    const RecompJob &j = jobs[i];
+    const int r = ranks[i];
+    if (r == 0) continue;
+    if (j.dense) {
+      cp.push_back(CopyDesc{work + j.jo_u, j.m, out + uo[i], j.m, j.m, r});
+      cp.push_back(CopyDesc{work + j.jo_v, j.n, out + vo[i], j.n, j.n, r});
+    } else {
+      int pu = gf.add(kOut, uo[i], j.m, j.m, r);
+      gf.seg(pu, kWork, j.u, j.m, 0, kWork, j.jo_u, j.S, 0, j.S);
+      int pv = gf.add(kOut, vo[i], j.n, j.n, r);
+      gf.seg(pv, kWork, j.v, j.n, 0, kWork, j.jo_v, j.S, 0, j.S);
+    }
+  }
+  run_copies(cp, s);
+  gemm_f64_run(gf, gb, TileShape::M128N64, s, false);
+}
+
 struct Term {        // one low-rank term of an output block
   int kind;          // 0 ancestor, 1 in-node "subtree x U_B", 2 in-node "U_A"
   int a_block, b_block;
@@ -175,36 +335,20 @@ std::shared_ptr<DeviceTree> hxh_multiply(DeviceTree &A, DeviceTree &B, double to
     ucat[b] = take((long long)o.m * std::max(S[b], 1));
     vcat[b] = take((long long)o.n * std::max(S[b], 1));
   }
-  // recompression workspaces
-  std::vector<char> dense(nb, 0);
-  std::vector<long long> ru(nb, 0), rv(nb, 0), mm(nb, 0), cs(nb, 0), jws(nb, 0), jo_u(nb, 0),
-      jo_v(nb, 0), jsig(nb, 0), dmat(nb, 0);
-  int max_c = 1;
+  // recompression jobs, one per output block
+  std::vector<RecompJob> jobs(nb);
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &o = ga.blocks[b];
+    RecompJob &j = jobs[b];
+    j.m = o.m;
+    j.n = o.n;
+    j.S = S[b];
+    j.u = ucat[b];
+    j.v = vcat[b];
     const int mn = std::min(o.m, o.n);
-    if (mn == 0) continue;
-    const int Sb = std::max(S[b], 1);
-    dense[b] = (S[b] >= mn && mn <= dense_max) ? 1 : 0;
-    if (dense[b]) {
-      dmat[b] = take((long long)o.m * o.n);
-      jws[b] = take(jacobi_workspace(o.m, o.n));
-      jo_u[b] = take((long long)o.m * mn);
-      jo_v[b] = take((long long)o.n * mn);
-      jsig[b] = take(mn);
-      max_c = std::max(max_c, mn);
-    } else {
-      ru[b] = take((long long)Sb * Sb);
-      rv[b] = take((long long)Sb * Sb);
-      mm[b] = take((long long)Sb * Sb);
-      cs[b] = take((long long)Sb * kPanel);
-      jws[b] = take(jacobi_workspace(Sb, Sb));
-      jo_u[b] = take((long long)Sb * Sb);
-      jo_v[b] = take((long long)Sb * Sb);
-      jsig[b] = take(Sb);
-      max_c = std::max(max_c, Sb);
-    }
+    j.dense = mn > 0 && S[b] >= mn && mn <= dense_max;
   }
+  const int max_c = recomp_layout(jobs, take);
   // diagonal leaves: products and ancestor intermediates T = U_A[rows] core
   std::vector<long long> leaf_out(nleaf), tmat;
   std::vector<std::vector<std::pair<int, long long>>> leaf_terms(nleaf);
@@ -302,84 +446,7 @@ std::shared_ptr<DeviceTree> hxh_multiply(DeviceTree &A, DeviceTree &B, double to
   }
 
   // ---- 4. recompression ----------------------------------------------------------------
-  std::vector<BlockQr> qr;
-  GemmBatch gd;   // dense products U V^T of the dense-path blocks
-  for (int b = 0; b < nb; ++b) {
-    const BlockDesc &o = ga.blocks[b];
-    if (std::min(o.m, o.n) == 0 || S[b] == 0) continue;
-    if (dense[b]) {
-      int p = gd.add(kWork, dmat[b], o.m, o.m, o.n);
-      gd.seg(p, kWork, ucat[b], o.m, 0, kWork, vcat[b], o.n, 1, S[b]);
-    } else {
-      qr.push_back(BlockQr{work + ucat[b], o.m, o.m, S[b], work + ru[b], S[b], work + cs[b]});
-      qr.push_back(BlockQr{work + vcat[b], o.n, o.n, S[b], work + rv[b], S[b], work + cs[b]});
-    }
-  }
-  gemm_f64_run(gd, gb, TileShape::M128N64, s);
-  // the two QRs of a block share its C scratch: run U's and V's separately
-  std::vector<BlockQr> qr_u, qr_v;
-  for (size_t i = 0; i < qr.size(); ++i) (i % 2 == 0 ? qr_u : qr_v).push_back(qr[i]);
-  block_qr(qr_u, work, s);
-  block_qr(qr_v, work, s);
-  {
-    GemmBatch gm;   // M = R_U R_V^T
-    for (int b = 0; b < nb; ++b) {
-      if (dense[b] || S[b] == 0 || std::min(ga.blocks[b].m, ga.blocks[b].n) == 0) continue;
-      int p = gm.add(kWork, mm[b], S[b], S[b], S[b]);
-      gm.seg(p, kWork, ru[b], S[b], 0, kWork, rv[b], S[b], 1, S[b]);
-    }
-    gemm_f64_run(gm, gb, TileShape::M64N128, s);
-  }
-  std::vector<JacobiProb> jp;
-  std::vector<int> jp_block;
-  int *d_int = nullptr;
-  HB_CUDA(cudaMallocAsync((void **)&d_int, sizeof(int) * (nb + 1), s));
-  HB_CUDA(cudaMemsetAsync(d_int, 0, sizeof(int) * (nb + 1), s));
-  for (int b = 0; b < nb; ++b) {
-    const BlockDesc &o = ga.blocks[b];
-    if (std::min(o.m, o.n) == 0 || S[b] == 0) continue;
-    JacobiProb p{};
-    p.transA = 0;
-    if (dense[b]) {
-      p.A = work + dmat[b];
-      p.lda = o.m;
-      p.m = o.m;
-      p.n = o.n;
-      p.ldu = o.m;
-      p.ldv = o.n;
-    } else {
-      p.A = work + mm[b];
-      p.lda = S[b];
-      p.m = S[b];
-      p.n = S[b];
-      p.ldu = S[b];
-      p.ldv = S[b];
-    }
-    const long long R = std::max(p.m, p.n), C = std::min(p.m, p.n);
-    p.G = work + jws[b];
-    p.W = p.G + align_up(R * C);
-    p.U = work + jo_u[b];
-    p.V = work + jo_v[b];
-    p.sigma = work + jsig[b];
-    p.rank = d_int + b;
-    p.sweeps = nullptr;
-    jp.push_back(p);
-    jp_block.push_back(b);
-  }
-  if (!jp.empty()) {
-    JacobiParams prm;
-    prm.tol = tol;
-    prm.trunc = Truncation::Absolute;
-    prm.scale_u = 1;
-    prm.max_sweeps = (int)option("jacobi_max_sweeps", 60);
-    JacobiProb *d_jp = upload_vec(jp, s);
-    jacobi_svd_batched(d_jp, (int)jp.size(), prm, d_int + nb, max_c, s);
-    cudaFreeAsync(d_jp, s);
-  }
-  std::vector<int> ints(nb + 1, 0);
-  HB_CUDA(cudaMemcpyAsync(ints.data(), d_int, sizeof(int) * (nb + 1), cudaMemcpyDeviceToHost, s));
-  HB_CUDA(cudaStreamSynchronize(s));
-  *status = ints[nb];
+  const std::vector<int> ranks = recomp_run(jobs, work, tol, max_c, s, status);
 
   // ---- 5. diagonal leaves ----------------------------------------------------------------
   {
@@ -412,35 +479,70 @@ std::shared_ptr<DeviceTree> hxh_multiply(DeviceTree &A, DeviceTree &B, double to
 
   // ---- 6. output tree ----------------------------------------------------------------------
   Geometry go = ga;
-  for (int b = 0; b < nb; ++b) go.blocks[b].s = (S[b] == 0) ? 0 : ints[b];
+  for (int b = 0; b < nb; ++b) go.blocks[b].s = ranks[b];
   std::shared_ptr<DeviceTree> out = dtree_create(go, s);
-  gb.p[kOut] = out->arena;
   std::vector<CopyDesc> cp;
   for (int i = 0; i < nleaf; ++i) {
     const int m = go.leaf_m[i];
     if (m) cp.push_back(CopyDesc{work + leaf_out[i], m, out->arena + out->leaves[i].off, m, m, m});
   }
-  GemmBatch gf;
-  for (int b = 0; b < nb; ++b) {
-    const BlockDesc &o = out->g.blocks[b];
-    if (o.s == 0) continue;
-    if (dense[b]) {
-      cp.push_back(CopyDesc{work + jo_u[b], o.m, out->arena + o.u_off, o.m, o.m, o.s});
-      cp.push_back(CopyDesc{work + jo_v[b], o.n, out->arena + o.v_off, o.n, o.n, o.s});
-    } else {
-      int pu = gf.add(kOut, o.u_off, o.m, o.m, o.s);
-      gf.seg(pu, kWork, ucat[b], o.m, 0, kWork, jo_u[b], S[b], 0, S[b]);
-      int pv = gf.add(kOut, o.v_off, o.n, o.n, o.s);
-      gf.seg(pv, kWork, vcat[b], o.n, 0, kWork, jo_v[b], S[b], 0, S[b]);
-    }
-  }
   run_copies(cp, s);
-  gemm_f64_run(gf, gb, TileShape::M128N64, s, false);
+  std::vector<long long> uo(nb), vo(nb);
+  for (int b = 0; b < nb; ++b) {
+    uo[b] = out->g.blocks[b].u_off;
+    vo[b] = out->g.blocks[b].v_off;
+  }
+  recomp_finish(jobs, ranks, work, out->arena, uo, vo, s);
   HB_CUDA(cudaStreamSynchronize(s));
-  dev_free(d_int, s);
   dev_free(work, s);
   HB_CUDA(cudaStreamSynchronize(s));
   return out;
+}
+
+int recompress_one(int m, int n, int S, const double *d_u, int ldu, const double *d_v, int ldv,
+                   double tol, bool dense, double *d_uo, double *d_vo, int *rank,
+                   cudaStream_t s) {
+  HB_REQUIRE(m >= 0 && n >= 0 && S >= 0 && ldu >= std::max(m, 1) && ldv >= std::max(n, 1),
+             INPUT_ERROR, "recompress: negative size or leading dimension below the rows");
+  *rank = 0;
+  if (std::min(m, n) == 0 || S == 0) return SUCCESS;
+  HB_REQUIRE(d_u && d_v && d_uo && d_vo, INPUT_ERROR, "recompress: NULL buffer");
+  long long ws = 0;
+  auto take = [&](long long e) {
+    const long long o = ws;
+    ws += align_up(std::max<long long>(e, 1));
+    return o;
+  };
+  std::vector<RecompJob> jobs(1);
+  RecompJob &j = jobs[0];
+  j.m = m;
+  j.n = n;
+  j.S = S;
+  j.dense = dense;
+  j.u = take((long long)m * S);
+  j.v = take((long long)n * S);
+  const int max_c = recomp_layout(jobs, take);
+  const int cap = std::max(S, std::min(m, n));
+  const long long uo = take((long long)m * cap), vo = take((long long)n * cap);
+  double *work = dev_alloc(ws, s);
+  HB_CUDA(cudaMemsetAsync(work, 0, ws * sizeof(double), s));
+  HB_CUDA(cudaMemcpy2DAsync(work + j.u, sizeof(double) * m, d_u, sizeof(double) * ldu,
+                            sizeof(double) * m, S, cudaMemcpyDeviceToDevice, s));
+  HB_CUDA(cudaMemcpy2DAsync(work + j.v, sizeof(double) * n, d_v, sizeof(double) * ldv,
+                            sizeof(double) * n, S, cudaMemcpyDeviceToDevice, s));
+  int status = SUCCESS;
+  const std::vector<int> ranks = recomp_run(jobs, work, tol, max_c, s, &status);
+  recomp_finish(jobs, ranks, work, work, {uo}, {vo}, s);
+  *rank = ranks[0];
+  if (ranks[0] > 0) {
+    HB_CUDA(cudaMemcpyAsync(d_uo, work + uo, sizeof(double) * (size_t)m * ranks[0],
+                            cudaMemcpyDeviceToDevice, s));
+    HB_CUDA(cudaMemcpyAsync(d_vo, work + vo, sizeof(double) * (size_t)n * ranks[0],
+                            cudaMemcpyDeviceToDevice, s));
+  }
+  HB_CUDA(cudaStreamSynchronize(s));
+  dev_free(work, s);
+  return status;
 }
 
 }  // namespace hb

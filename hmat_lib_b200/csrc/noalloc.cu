@@ -36,14 +36,45 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 double *g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
-// W offset of every block: exclusive prefix sum of the ranks.
-__global__ void noalloc_offsets_kernel(const BlockDesc *__restrict__ blocks, int nblocks,
-                                       int *__restrict__ woff) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int acc = 0;
-  for (int b = 0; b < nblocks; ++b) {
-    woff[b] = acc;
-    acc += blocks[b].s;
+// W offset of every block: exclusive prefix sum of the ranks, by one CTA of
+// 1024 threads (four blocks per thread, warp scans, then a scan of the warp
+// totals).  nblocks <= kNoAllocBlocks = 4096.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads)
+noalloc_offsets_kernel(const BlockDesc *__restrict__ blocks, int nblocks, int *__restrict__ woff) {
+  __shared__ int warp_total[kScanThreads / 32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  int v[4], local = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int b = 4 * t + q;
+    v[q] = b < nblocks ? blocks[b].s : 0;
+    local += v[q];
+  }
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_total[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int w = warp_total[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    warp_total[lane] = w;                 // inclusive totals of warps 0..lane
+  }
+  __syncthreads();
+  int acc = incl - local + (wid > 0 ? warp_total[wid - 1] : 0);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int b = 4 * t + q;
+    if (b < nblocks) woff[b] = acc;
+    acc += v[q];
   }
 }
 
@@ -71,14 +102,15 @@ __global__ void noalloc_rows_kernel(const LeafDesc *__restrict__ leaves,
                                     const BlockDesc *__restrict__ blocks, int height,
                                     const double *__restrict__ arena,
                                     const double *__restrict__ x, const int *__restrict__ woff,
-                                    const double *__restrict__ w, double *__restrict__ y) {
+                                    const double *__restrict__ w, int any_rank,
+                                    double *__restrict__ y) {
   const int i = blockIdx.x;
   const LeafDesc L = leaves[i];
   const double *D = arena + L.off;
   for (int r = threadIdx.x; r < L.m; r += blockDim.x) {
     double acc = 0.0;
     for (int c = 0; c < L.m; ++c) acc = fma(D[r + (long long)c * L.m], x[L.r0 + c], acc);
-    for (int d = height - 1; d >= 0; --d) {
+    for (int d = any_rank ? height - 1 : -1; d >= 0; --d) {
       const int j = i >> (height - d);
       const bool top = ((i >> (height - d - 1)) & 1) == 0;
       const int b = 2 * ((1 << d) - 1 + j) + (top ? 0 : 1);
@@ -91,18 +123,32 @@ __global__ void noalloc_rows_kernel(const LeafDesc *__restrict__ leaves,
   }
 }
 
-// Address of the scratch array on the current device; the first call on a
-// device looks it up (and must therefore come before any stream capture).
-double *scratch_for_current_device() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+// Address of the scratch array on device `dev`, which must be the current
+// device: the first call on a device looks it up (and must therefore come
+// before any stream capture).
+double *scratch_for_device(int dev) {
+  if (dev < 0 || dev >= kMaxDevices) return nullptr;
   std::lock_guard<std::mutex> lk(g_scratch_mutex);
   if (g_scratch_addr[dev] == nullptr) {
     double *ptr = nullptr;
-    if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch) != cudaSuccess) return nullptr;
+    if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return nullptr;
+    }
     g_scratch_addr[dev] = ptr;
   }
   return g_scratch_addr[dev];
+}
+
+// After a launch: a configuration error is this call's failure.
+bool launch_failed() {
+  count_launch();
+  return cudaGetLastError() != cudaSuccess;
+}
+
+int launch_error() {
+  set_last_error_static("hodlr_b200_matvec_noalloc_dev: kernel launch failed");
+  return HODLR_B200_CUDA_ERROR;
 }
 
 }  // namespace
@@ -112,7 +158,23 @@ extern "C" int hodlr_b200_matvec_noalloc_dev(hodlr_b200_tree t, const double *d_
                                              void *stream) {
   using namespace hb;
   if (!t || !t->p || !d_x || !d_y) return INPUT_ERROR;
+  // A CUDA error left behind by earlier asynchronous work (cudaGetLastError
+  // also clears it) is reported as such rather than as a failure of this call.
+  if (cudaGetLastError() != cudaSuccess) {
+    set_last_error_static(
+        "hodlr_b200_matvec_noalloc_dev: a CUDA error from earlier work was pending (now "
+        "cleared); nothing was launched");
+    return HODLR_B200_CUDA_ERROR;
+  }
   const DeviceTree &T = *t->p;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != T.device) {
+    (void)cudaGetLastError();
+    set_last_error_static(
+        "hodlr_b200_matvec_noalloc_dev: the current device is not the device that holds the "
+        "tree; make it current (cudaSetDevice) before the call");
+    return INPUT_ERROR;
+  }
   const Geometry &g = T.g;
   const int nblocks = g.nblock();
   long long total = 0;
@@ -128,29 +190,33 @@ extern "C" int hodlr_b200_matvec_noalloc_dev(hodlr_b200_tree t, const double *d_
     return INPUT_ERROR;
   }
   if (g.n == 0) return SUCCESS;
-  double *scratch = scratch_for_current_device();
+  double *scratch = scratch_for_device(dev);
   if (scratch == nullptr) {
-    set_last_error_static("hodlr_b200_matvec_noalloc_dev: cudaGetSymbolAddress failed");
-    return ALLOCATION_FAILURE;
+    set_last_error_static(
+        "hodlr_b200_matvec_noalloc_dev: cudaGetSymbolAddress of the fixed scratch failed");
+    return HODLR_B200_CUDA_ERROR;
   }
   double *w = scratch;
   int *woff = reinterpret_cast<int *>(scratch + kNoAllocW);
   cudaStream_t s = (cudaStream_t)stream;
-  if (nblocks > 0) {
-    noalloc_offsets_kernel<<<1, 32, 0, s>>>(T.d_blocks, nblocks, woff);
-    count_launch();
-    if (max_s > 0) {
+  if (max_s > 0) {
+    noalloc_offsets_kernel<<<1, kScanThreads, 0, s>>>(T.d_blocks, nblocks, woff);
+    if (launch_failed()) return launch_error();
+    {
       dim3 grid(nblocks, (max_s + 7) / 8);
       noalloc_project_kernel<<<grid, 256, 0, s>>>(T.d_blocks, T.arena, d_x, woff, w);
-      count_launch();
+      if (launch_failed()) return launch_error();
     }
   }
-  noalloc_rows_kernel<<<g.nleaf(), 256, 0, s>>>(T.d_leaves, T.d_blocks, g.h, T.arena, d_x, woff,
-                                                w, d_y);
-  count_launch();
-  if (cudaGetLastError() != cudaSuccess) {
-    set_last_error_static("hodlr_b200_matvec_noalloc_dev: kernel launch failed");
-    return ALLOCATION_FAILURE;
+  {
+    // one thread per leaf row: as many threads as the largest leaf has rows
+    // (rounded to whole warps, at most 256; longer leaves loop)
+    int max_m = 1;
+    for (int m : g.leaf_m) max_m = m > max_m ? m : max_m;
+    const int threads = max_m >= 256 ? 256 : (max_m + 31) / 32 * 32;
+    noalloc_rows_kernel<<<g.nleaf(), threads, 0, s>>>(T.d_leaves, T.d_blocks, g.h, T.arena, d_x,
+                                                      woff, w, max_s > 0 ? 1 : 0, d_y);
+    if (launch_failed()) return launch_error();
   }
   return SUCCESS;
 }

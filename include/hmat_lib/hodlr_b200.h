@@ -31,6 +31,10 @@ enum HodlrB200Op {
   HODLR_B200_OP_L = 2    /* Y = X H   (X is k x n) */
 };
 
+/* Status of the entry points that say so when a CUDA runtime call or a kernel
+ * launch fails (hmat_lib's ErrorCode has no such value). */
+enum { HODLR_B200_CUDA_ERROR = 100 };
+
 enum HodlrB200Precision {
   HODLR_B200_FP64 = 0,   /* FP64 DFMA products */
   HODLR_B200_MIXED = 1   /* split-precision tensor-core products with FP64 result */
@@ -39,11 +43,47 @@ enum HodlrB200Precision {
 const char *hodlr_b200_version(void);
 /* Message describing the last failure on the calling thread. */
 const char *hodlr_b200_last_error(void);
-/* Runtime knobs, e.g. "jacobi_max_sweeps". Returns SUCCESS.  "pool_keep"
- * (default 1): freed stream-ordered scratch stays mapped in the device's
- * default memory pool (release threshold unlimited) instead of being returned
- * at every synchronisation; set it to 0 before the library's first call on a
- * device to leave that pool's configuration untouched. */
+/* Runtime knobs (process-wide; read when a call or a cached plan is made).
+ * Returns SUCCESS.  Every option the library reads, with its default:
+ *   matmat_precision (0): 1 = host-buffer H X (multiply_hodlr_dense) on the
+ *       int8 tensor-core path
+ *   host_chunks (0): column chunks of host-buffer products; 0 automatic (up to
+ *       4 from 128 columns), 1 one piece, n that many
+ *   matvec_kernels (1): one right-hand side by the dedicated matvec kernels;
+ *       0 = the GEMM engine
+ *   pool_keep (1): freed stream-ordered scratch and tree arenas stay mapped in
+ *       the device's default memory pool (release threshold unlimited); set
+ *       0 before the library's first call on a device to leave that pool alone
+ *   learned_ranks (0): size each sketch from the rank model (fallback to
+ *       adaptive growth per block)
+ *   learned_margin (0.1), learned_extra (40), learned_eta (1.0): one-shot width
+ *       ceil((1 + margin) r) + extra; accepted when the residual estimate is
+ *       at most eta tol sigma_0
+ *   kernel_length (0): kernel length scale given to the rank model (0 unknown)
+ *   record_features (0): record per-block features and Frobenius eps-ranks of
+ *       the next builds (hodlr_b200_build_features)
+ *   sketch_first (64), sketch_step (64): first and later widths of the
+ *       adaptive range finder's rounds
+ *   sketch_eta (0.01): stopping residual, times tol sigma_0
+ *   sketch_cap (1024): largest sketch width (a block that needs more ends the
+ *       build with SVD_FAILURE)
+ *   sketch_seed (20240607): seed of the Gaussian test matrices
+ *   sketch_clean_rel (1e-13): rounding level below which a new panel is zeroed
+ *   exact_max (128): blocks with min(m, n) up to this are compressed by an
+ *       exact Jacobi SVD
+ *   jacobi_max_sweeps (60): Jacobi sweep bound (SVD_FAILURE past it)
+ *   jacobi_cluster_min_c (192): problems this wide or wider use a cluster of
+ *       8 CTAs
+ *   hxh_dense_max (256): H x H blocks up to this many rows are recompressed
+ *       from their dense product
+ *   autotune (1), batch_shape (-1), use_graphs (1), check_status (0): batched
+ *       products time candidate tile shapes / force one (0-3) / replay a CUDA
+ *       graph / read the mixed kernels' status word after each call
+ *   ozaki_schedule (1): int8 GEMM tile schedule, longest first (0 round-robin)
+ *   ozaki_phase1_tiles_per_cta (2): K-split granularity of the projections
+ *   ozaki_copy_split (1): bulk copies per int8 operand block
+ *   record_phase_times (0): events around each product phase and its main GEMM
+ *       (hodlr_b200_phase_times) */
 int hodlr_b200_set_option(const char *name, double value);
 /* Allocator for every host buffer the library allocates (tree nodes, factor
  * copies, results returned for out == NULL).  Both NULL restores malloc/free. */
@@ -94,6 +134,20 @@ int hodlr_b200_build_kernel_dev(int height, int n, const int *ms, const double *
                                 int dim, int kind, double length, double diag,
                                 double svd_threshold, int flags, void *stream,
                                 hodlr_b200_tree *out, int *ierr);
+/* Recompression of one low-rank product U V^T (U m x s, V n x s, device,
+ * column-major with leading dimensions ldu >= m, ldv >= n) by the routine
+ * hodlr_b200_hxh_dev / multiply_hodlr_hodlr applies to every output block.
+ * It replaces hmat_lib's internal recompress (src/hodlr_algebra.c:97-211):
+ * Householder QR of U and V, SVD of R_U R_V^T, absolute truncation of the
+ * singular values at svd_threshold (:160-163), U' = Q_U W Sigma, V' = Q_V Z;
+ * with dense != 0 it replaces recompress_large_s (:280-343), the SVD of the
+ * dense U V^T.  Writes the rank r to *rank and U' (m x r, ld m), V' (n x r,
+ * ld n) to d_u_out / d_v_out, which hold max(s, min(m, n)) columns.
+ * Synchronises with `stream`; returns an ErrorCode (SVD_FAILURE when the
+ * Jacobi SVD runs out of sweeps). */
+int hodlr_b200_recompress_dev(int m, int n, int s, const double *d_u, int ldu, const double *d_v,
+                              int ldv, double svd_threshold, int dense, double *d_u_out,
+                              double *d_v_out, int *rank, void *stream);
 /* Kernel matrix in device memory: out_ij = k(|p_i - p_j|) + diag delta_ij,
  * points column-major n x dim (coordinate a of point i at d_points[i + a n]);
  * kind 0: exp(-r^2 / (2 l^2)), 1: Matern-3/2 (1 + sqrt(3) r / l) exp(-sqrt(3) r / l),
@@ -125,10 +179,13 @@ int hodlr_b200_build_stats(double *out, int capacity);
  * (held on every GPU that loads it, until exit) instead of a per-call
  * allocation.  Limits: the ranks of the tree sum to at most 65536 and it has
  * at most 4096 off-diagonal blocks; larger trees return INPUT_ERROR with a
- * message.  The first call on a device looks the array's address up
+ * message.  The tree's device must be the current device (INPUT_ERROR
+ * otherwise).  The first call on a device looks the array's address up
  * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
  * share the array: calls that overlap on the GPU (unordered streams) race;
- * order them on one stream.  Returns an ErrorCode. */
+ * order them on one stream.  Returns an ErrorCode, or HODLR_B200_CUDA_ERROR
+ * when a launch fails or a CUDA error from earlier work was pending (that
+ * error is cleared and named in hodlr_b200_last_error()). */
 int hodlr_b200_matvec_noalloc_dev(hodlr_b200_tree t, const double *d_x, double *d_y,
                                   void *stream);
 /* Re-upload a host tree whose factor values were edited in place. */

@@ -1,6 +1,7 @@
 """The runtime options the library reads (option("name", default) in its C++
-and CUDA sources) and the options table of the integration guide name the
-same set, so a new or renamed option cannot go undocumented."""
+and CUDA sources) and the option list documented beside
+hodlr_b200_set_option in include/hmat_lib/hodlr_b200.h name the same set, so
+a new or renamed option cannot go undocumented."""
 import os
 import re
 
@@ -18,15 +19,13 @@ def _source_options():
 
 
 def _documented_options():
-    with open(os.path.join(ROOT, "INTEGRATION.md")) as fh:
+    with open(os.path.join(ROOT, "include", "hmat_lib", "hodlr_b200.h")) as fh:
         text = fh.read()
-    table = text.split("## Runtime options", 1)[1].split("\n## ", 1)[0]
-    names = set()
-    for line in table.splitlines():
-        if line.startswith("| `"):
-            first_cell = line.split("|")[1]
-            names |= set(re.findall(r"`([a-z_0-9]+)`", first_cell))
-    return names
+    block = text.split("Every option the library reads", 1)[1]
+    block = block.split("*/", 1)[0]
+    # entries: "name (default)" at the start of a documentation line or after
+    # a comma inside it
+    return set(re.findall(r"(?:^ \*   |, )([a-z][a-z_0-9]+) \(", block, flags=re.M))
 
 
 def test_every_option_is_documented_and_exists():

@@ -5,8 +5,10 @@ cannot take cudaMalloc's implicit device synchronisation).  Its scratch is a
 fixed array of device memory inside the library.
 
 Checked through the C-ABI against the existing device product
-(hodlr_b200_matmat_dev with one right-hand side) on two calls in a row, and
-for the clear rejection of a tree beyond the array's capacity.  Self-contained
+(hodlr_b200_matmat_dev with one right-hand side) on two calls in a row, on
+a single-leaf tree and on a tree whose blocks all have rank zero, and for the
+clear rejection of trees beyond the array's capacity (too many ranks, too
+many blocks) before anything is launched.  Self-contained
 so it passes alone in a fresh process and after the other tests."""
 import ctypes as C
 
@@ -89,5 +91,74 @@ def test_noalloc_matvec_rejects_tree_beyond_capacity():
     assert _noalloc(lib, dt, x, y, 0) == abi.INPUT_ERROR
     assert b"65536" in lib.hodlr_b200_last_error()
     assert float(y.abs().max()) == 0.0   # nothing launched
+    dt.free()
+    tree.free()
+
+
+def _random_tree(sizes, h, rank_of, seed=0):
+    rng = np.random.default_rng(seed)
+    td = TreeData(h, sizes, [rng.standard_normal((s, s)) for s in sizes])
+    for d in range(h):
+        for j in range(1 << d):
+            o, size, top = td.node_range(d, j)
+            r = rank_of(d, top)
+            for c in (1, 2):
+                m, nn = (top, size - top) if c == 1 else (size - top, top)
+                td.blocks[(d, j, c)] = (rng.standard_normal((m, r)), rng.standard_normal((nn, r)))
+    return td
+
+
+@pytest.mark.parametrize("case", ["single_leaf", "zero_ranks"])
+def test_noalloc_matvec_edge_trees(case):
+    """A tree of height 0 (one dense leaf, no off-diagonal block) and a tree
+    whose blocks all have rank 0 (no projection is launched): same result as
+    the existing device product and as the CPU oracle."""
+    import torch
+
+    lib = abi.load()
+    if case == "single_leaf":
+        n, h = 200, 0
+        td = _random_tree([n], h, lambda d, top: 0, seed=1)
+    else:
+        n, h = 1000, 3
+        td = _random_tree(O.block_sizes_halves(n, h), h, lambda d, top: 0, seed=2)
+    tree = Tree.from_tree_data(td)
+    dt = DeviceTree.of_host(tree)
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    y_ref = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    dt.matmat(x.data_ptr(), 1, n, y_ref.data_ptr(), n)
+    for _ in range(2):
+        y = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        assert _noalloc(lib, dt, x, y, 0) == abi.SUCCESS, lib.hodlr_b200_last_error()
+        torch.cuda.synchronize()
+        assert O.rel_fro(y.cpu().numpy(), y_ref.cpu().numpy()) < REL
+    want = O.multiply_dense(td, x.cpu().numpy())
+    assert O.rel_fro(y.cpu().numpy(), want) < REL
+    dt.free()
+    tree.free()
+
+
+def test_noalloc_matvec_rejects_too_many_blocks():
+    """Height 12 has 8190 off-diagonal blocks, past the 4096 offsets the fixed
+    scratch holds: INPUT_ERROR and a message before any launch (ranks tiny,
+    so only the block count is over)."""
+    import torch
+
+    lib = abi.load()
+    h = 12
+    n = 2 << h                      # leaves of 2 rows
+    td = _random_tree(O.block_sizes_halves(n, h), h, lambda d, top: 0, seed=3)
+    tree = Tree.from_tree_data(td)
+    dt = DeviceTree.of_host(tree)
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    launches = lib.hodlr_b200_kernel_launches()
+    assert _noalloc(lib, dt, x, y, 0) == abi.INPUT_ERROR
+    assert lib.hodlr_b200_kernel_launches() == launches
+    assert b"4096" in lib.hodlr_b200_last_error()
+    assert float(y.abs().max()) == 0.0
     dt.free()
     tree.free()
