@@ -1,16 +1,21 @@
-"""Generates tests/golden/ref_matern2d_n32768.npz: hmat_lib's own FP64 result
-on the full-size single-tree workload (run from the repo root, CPU only):
+"""Generates the full-size reference fixtures of tests/golden/ (run from the
+repo root, CPU only): hmat_lib's own FP64 results on two workloads.
 
     make -C oracle ref64
-    python tests/golden/make_ref_n32768.py [--threads 8]
+    python tests/golden/make_ref_fixtures.py --workload matern2d_n32768 [--threads 8]
+    python tests/golden/make_ref_fixtures.py --workload exp3d_n8192 [--threads 8]
 
-Workload: n = 32768 points of [0,1]^2 (seed 1) in Morton order, Matern-3/2
-kernel with length 0.1 plus 1e-2 I, HODLR depth 8 (leaf 128), truncation
-tolerance 1e-8.  The unmodified reference cannot build this size (its
-constructor computes scratch sizes and block offsets in `int`, hmat_lib
-src/constructors.c:464, 676), so this runs the copy "patched for 64-bit
-sizes" that oracle/Makefile's `ref64` target builds: the same code with only
-those integers widened.
+matern2d_n32768 -> ref_matern2d_n32768.npz: n = 32768 points of [0,1]^2
+    (seed 1) in Morton order, Matern-3/2 kernel with length 0.1 plus 1e-2 I,
+    depth 8 (leaf 128), tolerance 1e-8.  The unmodified reference cannot
+    build this size (its constructor computes scratch sizes and block offsets
+    in `int`, hmat_lib src/constructors.c:464, 676), so this runs the copy
+    "patched for 64-bit sizes" that oracle/Makefile's `ref64` target builds:
+    the same code with only those integers widened.
+exp3d_n8192 -> ref_exp3d_n8192.npz: n = 8192 points of [0,1]^3 (seed 4) in
+    Morton order, exp(-r / 0.15) plus 1e-2 I, depth 6 (leaf 128), tolerance
+    1e-8 -- the family of the n = 65536 learned-rank workload at a size the
+    unmodified reference builds.
 
 Stored: the rank of every off-diagonal block (order b = 2(2^d - 1 + j) +
 (c - 1), as DeviceTree.ranks() returns them), the reference's
@@ -37,8 +42,15 @@ sys.path.insert(0, ROOT)
 from hmat_lib_b200 import abi, workloads as W  # noqa: E402
 from hmat_lib_b200.tree import node_at  # noqa: E402
 
-OUT = os.path.join(HERE, "ref_matern2d_n32768.npz")
+REF = os.path.join(ROOT, "oracle", "_ref", "libhmat_ref.so")
 REF64 = os.path.join(ROOT, "oracle", "_ref", "libhmat_ref64.so")
+FIXTURES = {
+    # workload: (n, dim, seed, kind, length, diag, height, library, label)
+    "matern2d_n32768": (32768, 2, 1, "matern32", 0.1, 1e-2, 8, REF64,
+                        "hmat_lib patched for 64-bit sizes (oracle/Makefile ref64)"),
+    "exp3d_n8192": (8192, 3, 4, "exponential", 0.15, 1e-2, 6, REF,
+                    "hmat_lib, unmodified (oracle/Makefile)"),
+}
 X_SEED = 7
 X_COLS = 4
 
@@ -69,14 +81,17 @@ def block_ranks(tp) -> np.ndarray:
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", choices=sorted(FIXTURES), default="matern2d_n32768")
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     ap.add_argument("--n", type=int, default=None, help="smaller n (trial runs only)")
-    ap.add_argument("--out", default=OUT)
+    ap.add_argument("--out", default=None)
     args = ap.parse_args()
+    n, dim, seed, kind, length, diag, h, libpath, label = FIXTURES[args.workload]
+    out_path = args.out or os.path.join(HERE, f"ref_{args.workload}.npz")
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
-    if not os.path.exists(REF64):
-        raise SystemExit(f"{REF64} missing: run make -C oracle ref64")
-    lib = abi.load_hmat_abi(REF64)
+    if not os.path.exists(libpath):
+        raise SystemExit(f"{libpath} missing: run make -C oracle (ref64 for the patched copy)")
+    lib = abi.load_hmat_abi(libpath)
     libgomp = C.CDLL("libgomp.so.1", mode=C.RTLD_GLOBAL)
     libgomp.omp_set_num_threads(C.c_int(args.threads))
     import sysconfig
@@ -88,13 +103,12 @@ def main():
     if blas is not None:
         blas.openblas_set_num_threads(C.c_int(1))
 
-    w = W.WORKLOADS["matern2d_n32768"]
-    n, h, tol = w["n"], w["height"], w["tol"]
+    tol = 1e-8
     if args.n is not None:
         n, h = args.n, max(1, (args.n // 128).bit_length() - 1)
-    pts = W.workload_points("matern2d_n32768", n)
+    pts = W.points_morton(n, dim, seed)
     t0 = time.perf_counter()
-    a = kernel_matrix_blocked(pts, w["kind"], w["length"], w["diag"])
+    a = kernel_matrix_blocked(pts, kind, length, diag)
     x = np.asfortranarray(W.rhs(n, X_COLS, seed=X_SEED))
     y_dense = a @ x
     print(f"matrix + dense product: {time.perf_counter() - t0:.1f} s", flush=True)
@@ -126,11 +140,10 @@ def main():
         if line.startswith("model name"):
             cpu = line.split(":", 1)[1].strip()
             break
-    meta = dict(workload="matern2d_n32768", n=n, height=h, tol=tol, x_seed=X_SEED, x_cols=X_COLS,
+    meta = dict(workload=args.workload, n=n, height=h, tol=tol, x_seed=X_SEED, x_cols=X_COLS,
                 build_s=build_s, matmat_s_4cols=matmat_s, threads=args.threads, cpu=cpu,
-                rel_err_ref_vs_dense=err, library="hmat_lib patched for 64-bit sizes "
-                "(oracle/Makefile ref64)")
-    np.savez_compressed(args.out, ranks=ranks, y_ref=y, meta=json.dumps(meta))
+                rel_err_ref_vs_dense=err, library=label)
+    np.savez_compressed(out_path, ranks=ranks, y_ref=y, meta=json.dumps(meta))
     print(json.dumps(meta))
     lib.free_tree_hodlr(C.byref(tp))
 
