@@ -1,6 +1,7 @@
 // FP64 variable-batched segmented GEMM for sm_100a.
 //
-// CUDA-core DFMA kernel: 256 threads, a BM x BN output tile per CTA
+// Two kernels (option gemm_f64_engine): the FP64 tensor-core (DMMA) kernel
+// (default, below), and a CUDA-core DFMA kernel: 256 threads, a BM x BN output tile per CTA
 // (128 x 64, 64 x 128, 32 x 128 or 32 x 256), K advanced 16 at a time through a two-stage
 // cp.async pipeline (8-byte copies with zero fill, so any leading dimension
 // and any offset work), 32 accumulators per thread, operands read from shared
@@ -13,6 +14,8 @@
 #include "gemm_f64.h"
 
 namespace hb {
+
+int gemm_f64_engine() { return (int)option("gemm_f64_engine", 1); }
 
 namespace {
 
@@ -209,6 +212,258 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
   }
 }
 
+// ---- FP64 tensor-core (DMMA) variant ------------------------------------------------
+// Same tiles, segments and K iteration as gemm_f64_kernel, with the multiply-adds
+// on the FP64 tensor-core path (mma.sync m8n8k4 .f64: one warp instruction is an
+// 8 x 8 x 4 product, 256 FMAs).  Eight warps per CTA, each owning a WM x WN
+// sub-tile of the BM x BN output (WM/8 x WN/8 MMA tiles, two accumulators per
+// lane each).  K advances 16 at a time through a cp.async ring.  Each operand
+// is staged in the layout that makes its global reads contiguous: an operand
+// whose contiguous dimension is K is stored [row][k] (16 + 4 doubles per
+// row), otherwise [k][row] (BM or BN + 4 per k); the pads make every fragment
+// load of a half-warp hit 16 distinct 8-byte bank pairs.  Copies are 16 bytes
+// when the operand's offset and leading dimension (and, for K-contiguous
+// operands, the first K index) are even, else 8; elements past M, N or the K
+// range are zero-filled.  The ring is as deep as two CTAs per SM allow (2 to
+// 4 stages).
+template <int BM, int BN>
+struct MmaSmem {
+  static constexpr int LDKM = BM + 4;      // [k][m] layout
+  static constexpr int LDKN = BN + 4;      // [k][n] layout
+  static constexpr int LDK = kBK + 4;      // [m][k] / [n][k] layout
+  static constexpr int A_ELEMS = (kBK * LDKM > BM * LDK) ? kBK * LDKM : BM * LDK;
+  static constexpr int B_ELEMS = (kBK * LDKN > BN * LDK) ? kBK * LDKN : BN * LDK;
+  static constexpr int STAGE = A_ELEMS + B_ELEMS;
+  static constexpr int STAGES_FIT = (int)(112 * 1024 / (sizeof(double) * STAGE));
+  static constexpr int STAGES = STAGES_FIT > 4 ? 4 : (STAGES_FIT < 2 ? 2 : STAGES_FIT);
+  static constexpr size_t bytes = sizeof(double) * STAGES * STAGE;
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+               "r"(src_bytes));
+}
+
+__device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+template <int BM, int BN, int WM, int WN>
+__global__ void __launch_bounds__(kThreads, 2)
+gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ probs,
+                    const GemmTile *__restrict__ tiles, GemmBases bases) {
+  using SM = MmaSmem<BM, BN>;
+  constexpr int kMmaStages = SM::STAGES;
+  constexpr int MT = WM / 8, NT = WN / 8;          // MMA tiles per warp
+  constexpr int WARPS_N = BN / WN;
+  static_assert((BM / WM) * (BN / WN) == kThreads / 32, "eight warps per CTA");
+  extern __shared__ __align__(16) double smem[];
+
+  const GemmTile tile = tiles[blockIdx.x];
+  const GemmProb P = probs[tile.prob];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp / WARPS_N) * WM, wn0 = (warp % WARPS_N) * WN;
+  const int seg_end = P.seg0 + P.nseg;
+
+  double acc[MT][NT][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  auto settle = [&](KIter &it) {
+    while (it.si < seg_end) {
+      const int K = segs[it.si].K;
+      const int ls = max(tile.k0 - it.kbase, 0);
+      const int le = min(tile.k1 - it.kbase, K);
+      if (ls < le) {
+        it.kk = ls;
+        it.le = le;
+        return;
+      }
+      it.kbase += K;
+      ++it.si;
+    }
+  };
+  auto advance = [&](KIter &it) {
+    it.kk += kBK;
+    if (it.kk >= it.le) {
+      it.kbase += segs[it.si].K;
+      ++it.si;
+      settle(it);
+    }
+  };
+
+  // One operand tile of `rows` lines (M or N side) x kBK into stage memory.
+  // `kcontig`: K is the contiguous dimension in global memory (stored
+  // [line][k] in shared memory), otherwise lines are ([k][line]).  Element
+  // (line, k) of the tile is global (row0 + line, kk + k) of the operand,
+  // stored at base + off + r + c ld with (r, c) = (line, k), or (k, line) when
+  // kcontig; lines >= nlines and k >= kend are zero.
+  auto load_operand = [&](double *dst, bool gen, const double *base, long long off, long long ld,
+                          bool kcontig, int rows, int row0, int nlines, int kk, int kend) {
+    if (gen) {
+      // generated kernel-matrix entries: (r, c) of the block at gen_offset(row0, col0)
+      const int gr0 = (int)(off >> 32), gc0 = (int)(off & 0xffffffffLL);
+      for (int e = tid; e < rows * kBK; e += kThreads) {
+        int line, k;
+        if (kcontig) {
+          line = e / kBK;
+          k = e % kBK;
+        } else {
+          k = e / rows;
+          line = e % rows;
+        }
+        const bool p = (row0 + line) < nlines && (kk + k) < kend;
+        double v = 0.0;
+        if (p) {
+          const int r = kcontig ? kk + k : row0 + line;
+          const int c = kcontig ? row0 + line : kk + k;
+          v = kernel_entry(bases.gen, gr0 + r, gc0 + c);
+        }
+        if (kcontig)
+          dst[line * SM::LDK + k] = v;
+        else
+          dst[k * (rows + 4) + line] = v;
+      }
+      return;
+    }
+    // 16-byte copies need even element offsets: the operand's offset and
+    // leading dimension, and for K-contiguous operands the first K index
+    const bool vec = ((off | ld | (kcontig ? kk : 0)) & 1) == 0 &&
+                     (((unsigned long long)base) & 15) == 0;
+    if (kcontig) {
+      // per line kBK contiguous K values: kBK / 2 chunks of 16 bytes
+      constexpr int CH = kBK / 2;
+      for (int e = tid; e < rows * CH; e += kThreads) {
+        const int line = e / CH, k = 2 * (e % CH);
+        const bool lok = (row0 + line) < nlines;
+        const int nk = lok ? min(2, max(0, kend - (kk + k))) : 0;
+        double *d = dst + line * SM::LDK + k;
+        const double *src = base + off + (long long)(row0 + line) * ld + (kk + k);
+        if (vec) {
+          cp_async16(d, nk > 0 ? src : base, 8 * nk);
+        } else {
+          cp_async8(d, nk > 0 ? src : base, nk > 0);
+          cp_async8(d + 1, nk > 1 ? src + 1 : base, nk > 1);
+        }
+      }
+    } else {
+      // per k, `rows` contiguous lines: rows / 2 chunks of 16 bytes
+      const int CH = rows / 2;
+      for (int e = tid; e < kBK * CH; e += kThreads) {
+        const int k = e / CH, line = 2 * (e % CH);
+        const bool kok = (kk + k) < kend;
+        const int nl = kok ? min(2, max(0, nlines - (row0 + line))) : 0;
+        double *d = dst + k * (rows + 4) + line;
+        const double *src = base + off + (row0 + line) + (long long)(kk + k) * ld;
+        if (vec) {
+          cp_async16(d, nl > 0 ? src : base, 8 * nl);
+        } else {
+          cp_async8(d, nl > 0 ? src : base, nl > 0);
+          cp_async8(d + 1, nl > 1 ? src + 1 : base, nl > 1);
+        }
+      }
+    }
+  };
+
+  // Stage `buf` <- K-block `it`; returns its layout bits (1: A stored [m][k],
+  // 2: B stored [n][k]).
+  auto load = [&](int buf, const KIter &it) -> int {
+    const GemmSeg S = segs[it.si];
+    const bool ga = S.abase == kGenSlot, gb = S.bbase == kGenSlot;
+    double *as = smem + buf * SM::STAGE;
+    double *bs = as + SM::A_ELEMS;
+    // op(A) is M x K: ta = 0 stores (m, k) at m + k lda (lines contiguous),
+    // ta = 1 stores it at k + m lda (K contiguous)
+    load_operand(as, ga, ga ? nullptr : bases.p[S.abase], S.a_off, S.lda, S.ta == 1, BM,
+                 tile.m0, P.M, it.kk, it.le);
+    // op(B) is K x N: tb = 0 stores (k, n) at k + n ldb (K contiguous),
+    // tb = 1 at n + k ldb (lines contiguous)
+    load_operand(bs, gb, gb ? nullptr : bases.p[S.bbase], S.b_off, S.ldb, S.tb == 0, BN,
+                 tile.n0, P.N, it.kk, it.le);
+    return (S.ta == 1 ? 1 : 0) | (S.tb == 0 ? 2 : 0);
+  };
+
+  // ring of kMmaStages buffers; `lay` keeps 2 layout bits per buffer
+  KIter it{P.seg0, 0, 0, 0};
+  settle(it);
+  unsigned lay = 0;
+#pragma unroll
+  for (int st = 0; st < kMmaStages - 1; ++st) {
+    if (it.si < seg_end) {
+      lay |= (unsigned)load(st, it) << (2 * st);
+      advance(it);
+    }
+    cp_async_commit();
+  }
+  int buf = 0;
+  KIter cit{P.seg0, 0, 0, 0};
+  settle(cit);
+  while (cit.si < seg_end) {
+    cp_async_wait<kMmaStages - 2>();
+    __syncthreads();
+    {
+      const int nb = (buf + kMmaStages - 1) % kMmaStages;
+      if (it.si < seg_end) {
+        lay = (lay & ~(3u << (2 * nb))) | ((unsigned)load(nb, it) << (2 * nb));
+        advance(it);
+      }
+      cp_async_commit();
+    }
+    const unsigned l = (lay >> (2 * buf)) & 3u;
+    const double *as = smem + buf * SM::STAGE;
+    const double *bs = as + SM::A_ELEMS;
+    // per-lane fragment addressing: A (m = g, k = t), B (k = t, n = g)
+    const int a_line_step = (l & 1) ? SM::LDK : 1;       // next m
+    const int a_k_step = (l & 1) ? 1 : SM::LDKM;          // next k
+    const int b_line_step = (l & 2) ? SM::LDK : 1;       // next n
+    const int b_k_step = (l & 2) ? 1 : SM::LDKN;
+    const double *ap = as + (wm0 + g) * a_line_step + t * a_k_step;
+    const double *bp = bs + (wn0 + g) * b_line_step + t * b_k_step;
+#pragma unroll
+    for (int k4 = 0; k4 < kBK / 4; ++k4) {
+      double a[MT], b[NT];
+#pragma unroll
+      for (int i = 0; i < MT; ++i) a[i] = ap[(8 * i) * a_line_step + 4 * k4 * a_k_step];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) b[j] = bp[(8 * j) * b_line_step + 4 * k4 * b_k_step];
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) dmma884(acc[i][j], a[i], b[j]);
+    }
+    buf = (buf + 1) % kMmaStages;
+    advance(cit);
+  }
+  cp_async_wait<0>();
+
+  double *C = bases.p[P.cbase] + P.c_off;
+#pragma unroll
+  for (int i = 0; i < MT; ++i) {
+    const int m = tile.m0 + wm0 + 8 * i + g;
+    if (m >= P.M) continue;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int n = tile.n0 + wn0 + 8 * j + 2 * t + h;
+        if (n >= P.N) continue;
+        double *c = C + m + (long long)n * P.ldc;
+        const double v = P.alpha * acc[i][j][h];
+        if (P.split > 1)
+          atomicAdd(c, v);
+        else
+          *c = (P.beta == 0.0) ? v : v + P.beta * (*c);
+      }
+    }
+  }
+}
+
 // beta pre-pass for problems whose tiles accumulate with atomics
 __global__ void gemm_scale_c_kernel(const GemmProb *__restrict__ probs, int nprobs,
                                     GemmBases bases) {
@@ -226,8 +481,21 @@ __global__ void gemm_scale_c_kernel(const GemmProb *__restrict__ probs, int npro
   }
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int WM, int WN>
 void launch_gemm(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stream) {
+  if (gemm_f64_engine() == 1) {
+    static bool configured = false;
+    const size_t smem = MmaSmem<BM, BN>::bytes;
+    if (!configured) {
+      HB_CUDA(cudaFuncSetAttribute(gemm_f64_mma_kernel<BM, BN, WM, WN>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured = true;
+    }
+    gemm_f64_mma_kernel<BM, BN, WM, WN><<<plan.ntiles, kThreads, smem, stream>>>(
+        plan.segs, plan.probs, plan.tiles, bases);
+    HB_LAUNCHED();
+    return;
+  }
   static bool configured = false;
   const size_t smem = Smem<BM, BN>::bytes;
   if (!configured) {
@@ -347,10 +615,10 @@ void gemm_plan_run(const GemmPlan &plan, const GemmBases &bases, cudaStream_t st
     HB_LAUNCHED();
   }
   switch (plan.shape) {
-    case TileShape::M128N64: launch_gemm<128, 64>(plan, bases, stream); break;
-    case TileShape::M64N128: launch_gemm<64, 128>(plan, bases, stream); break;
-    case TileShape::M32N128: launch_gemm<32, 128>(plan, bases, stream); break;
-    case TileShape::M32N256: launch_gemm<32, 256>(plan, bases, stream); break;
+    case TileShape::M128N64: launch_gemm<128, 64, 32, 32>(plan, bases, stream); break;
+    case TileShape::M64N128: launch_gemm<64, 128, 32, 32>(plan, bases, stream); break;
+    case TileShape::M32N128: launch_gemm<32, 128, 32, 16>(plan, bases, stream); break;
+    case TileShape::M32N256: launch_gemm<32, 256, 32, 32>(plan, bases, stream); break;
   }
 }
 

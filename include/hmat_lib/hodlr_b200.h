@@ -83,7 +83,9 @@ const char *hodlr_b200_last_error(void);
  *   ozaki_phase1_tiles_per_cta (2): K-split granularity of the projections
  *   ozaki_copy_split (1): bulk copies per int8 operand block
  *   record_phase_times (0): events around each product phase and its main GEMM
- *       (hodlr_b200_phase_times) */
+ *       (hodlr_b200_phase_times)
+ *   gemm_f64_engine (1): FP64 products on the FP64 tensor cores (DMMA); 0 =
+ *       the DFMA kernel */
 int hodlr_b200_set_option(const char *name, double value);
 /* Allocator for every host buffer the library allocates (tree nodes, factor
  * copies, results returned for out == NULL).  Both NULL restores malloc/free. */
