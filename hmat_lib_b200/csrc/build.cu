@@ -155,7 +155,10 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
   cudaFreeAsync(d_jp, stream);
   cudaFreeAsync(d_rank, stream);
   dev_free(w, stream);
-  const double length = option("kernel_length", 0.0);
+  // kernel length scale: option kernel_length, else (matrix-free build) the
+  // length of the kernel being compressed, else unknown (feature 0)
+  double length = option("kernel_length", 0.0);
+  if (length <= 0.0 && aslot == (int)kGenSlot) length = gen.length;
   for (int i = 0; i < nsk; ++i) {
     const SketchBlock &S = sk[i];
     float *row = &f[(size_t)i * kRankIn];
@@ -185,7 +188,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   const int nb = g.nblock();
   *svd_status = SUCCESS;
   const int exact_max = (int)option("exact_max", 128);
-  const int cap_max = (int)option("sketch_cap", 1024) / kPanel * kPanel;
+  const int cap_opt = (int)option("sketch_cap", 0.0) / kPanel * kPanel;
   const int w_first = std::max(kPanel, (int)option("sketch_first", 64) / kPanel * kPanel);
   const int w_next = std::max(kPanel, (int)option("sketch_step", 64) / kPanel * kPanel);
   const double eta = option("sketch_eta", 0.01);
@@ -224,14 +227,71 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     eslots.push_back(s);
     max_c = std::max(max_c, C);
   }
+  // Sketch width caps.  Option sketch_cap > 0 fixes one cap for every block;
+  // 0 (default) bounds them by memory: every sketched block may grow to
+  // alpha min(m, n) columns (whole panels, at least two rounds' width), with
+  // alpha in (0, 1] the largest value whose scratch -- Q, B^T, P, R_B and the
+  // round buffers, plus the SVD of the core -- fits option sketch_mem_frac
+  // (default 0.6) of the device memory that is free or held unused by the
+  // stream-ordered pool.
+  std::vector<int> caps(sketched.size(), 0);
+  {
+    const int w_round = std::max(w_first, w_next);
+    auto cap_of = [&](const BlockDesc &B, double alpha) {
+      const int C = std::min(B.m, B.n);
+      if (cap_opt > 0) return std::min(C, std::max(cap_opt, kPanel));
+      const int c = (int)std::ceil(alpha * C / kPanel) * kPanel;
+      return std::min(C, std::max(c, 2 * w_round));
+    };
+    auto bytes_of = [&](double alpha) {
+      double total = 0.0;
+      for (int b : sketched) {
+        const BlockDesc &B = g.blocks[b];
+        const double c = cap_of(B, alpha);
+        // q, bt, p, rb, om, t, c, rn, and the core SVD's G, W, U, V
+        total += 8.0 * ((double)B.m * c + 2.0 * B.n * c + c * c + (double)B.n * w_round +
+                        c * w_round + c * kPanel + 2.0 * kPanel * kPanel + 4.0 * c * c);
+      }
+      return total;
+    };
+    double alpha = 1.0;
+    if (cap_opt <= 0) {
+      size_t free_b = 0, total_b = 0;
+      HB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      double avail = (double)free_b;
+      int dev = 0;
+      cudaMemPool_t pool;
+      if (cudaGetDevice(&dev) == cudaSuccess &&
+          cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t reserved = 0, used = 0;
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
+                cudaSuccess &&
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+            reserved > used)
+          avail += (double)(reserved - used);
+      }
+      (void)cudaGetLastError();
+      const double budget = option("sketch_mem_frac", 0.6) * avail;
+      if (bytes_of(1.0) > budget) {
+        double lo = 0.0, hi = 1.0;
+        for (int it = 0; it < 40; ++it) {
+          const double mid = 0.5 * (lo + hi);
+          (bytes_of(mid) <= budget ? lo : hi) = mid;
+        }
+        alpha = lo;
+      }
+    }
+    for (size_t i = 0; i < sketched.size(); ++i) caps[i] = cap_of(g.blocks[sketched[i]], alpha);
+  }
   std::vector<SketchBlock> sk;
-  for (int b : sketched) {
+  for (size_t si = 0; si < sketched.size(); ++si) {
+    const int b = sketched[si];
     const BlockDesc &B = g.blocks[b];
     SketchBlock S;
     S.b = b;
     S.m = B.m;
     S.n = B.n;
-    S.cap = std::min(std::min(B.m, B.n), std::max(cap_max, kPanel));
+    S.cap = caps[si];
     S.a_off = gen ? gen_offset(B.r0, B.c0) : B.r0 + (long long)B.c0 * lda;
     sk.push_back(S);
   }
@@ -703,7 +763,10 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   HB_CUDA(cudaStreamSynchronize(stream));
   if (cap_hit) {
     *svd_status = SVD_FAILURE;
-    set_last_error("a block's rank reached the sketch cap (option sketch_cap)");
+    set_last_error(cap_opt > 0
+                       ? "a block's rank reached the sketch cap (option sketch_cap)"
+                       : "a block's rank reached the sketch width that fits the device memory "
+                         "(option sketch_mem_frac)");
   }
   BuildStats st;
   st.exact_blocks = (int)exact.size();

@@ -59,14 +59,18 @@ const char *hodlr_b200_last_error(void);
  *   learned_margin (0.1), learned_extra (40), learned_eta (1.0): one-shot width
  *       ceil((1 + margin) r) + extra; accepted when the residual estimate is
  *       at most eta tol sigma_0
- *   kernel_length (0): kernel length scale given to the rank model (0 unknown)
+ *   kernel_length (0): kernel length scale given to the rank model (0: the
+ *       kernel's own length in a matrix-free build, else unknown)
  *   record_features (0): record per-block features and Frobenius eps-ranks of
  *       the next builds (hodlr_b200_build_features)
  *   sketch_first (64), sketch_step (64): first and later widths of the
  *       adaptive range finder's rounds
  *   sketch_eta (0.01): stopping residual, times tol sigma_0
- *   sketch_cap (1024): largest sketch width (a block that needs more ends the
- *       build with SVD_FAILURE)
+ *   sketch_cap (0): largest sketch width (a block that needs more ends the
+ *       build with SVD_FAILURE); 0 = as wide as memory allows
+ *   sketch_mem_frac (0.6): with sketch_cap 0, the share of the free device
+ *       memory (including memory the stream-ordered pool holds unused) that
+ *       the build's sketches may take
  *   sketch_seed (20240607): seed of the Gaussian test matrices
  *   sketch_clean_rel (1e-13): rounding level below which a new panel is zeroed
  *   exact_max (128): blocks with min(m, n) up to this are compressed by an
