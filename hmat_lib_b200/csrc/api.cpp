@@ -127,14 +127,14 @@ void host_product(DeviceTree &t, ProdOp op, const double *X, long long xr, long 
                   long long ldx, double *Y, long long ldy) {
   cudaStream_t s = lib_stream();
   DevBuf dx(xr * xc, s), dy(xr * xc, s);
-  // option "matmat_precision" = 1 routes H X through the int8 tensor-core
-  // path (about 42 bits); the default keeps FP64 throughout
+  // option "matmat_precision" = 1 routes H X, H^T X and X H through the int8
+  // tensor-core path (about 42 bits); the default keeps FP64 throughout
   bool aligned = true;
   for (int m : t.g.leaf_m) aligned = aligned && (m % 32 == 0);
-  const bool mixed = op == ProdOp::N && aligned && option("matmat_precision", 0.0) == 1.0;
+  const bool mixed = aligned && option("matmat_precision", 0.0) == 1.0;
   auto product = [&](const double *xd, double *yd, int k) {
     if (mixed)
-      product_mixed(t, xd, k, xr, yd, xr, s);
+      product_mixed_op(t, op, xd, k, xr, yd, xr, s);
     else
       product_f64(t, op, xd, k, xr, yd, xr, s);
   };
@@ -582,9 +582,7 @@ int hodlr_b200_matmat_dev(hodlr_b200_tree t, int op, int precision, const double
     HB_REQUIRE(k >= 0 && ldx >= std::max(1LL, rows) && ldy >= std::max(1LL, rows), INPUT_ERROR,
                "leading dimension below the number of rows");
     if (precision == HODLR_B200_MIXED) {
-      HB_REQUIRE(op == HODLR_B200_OP_N, INPUT_ERROR,
-                 "mixed precision is available for Y = H X (op N)");
-      product_mixed(*t->p, d_x, k, ldx, d_y, ldy, as_stream(stream));
+      product_mixed_op(*t->p, (ProdOp)op, d_x, k, ldx, d_y, ldy, as_stream(stream));
       return SUCCESS;
     }
     HB_REQUIRE(precision == HODLR_B200_FP64, INPUT_ERROR, "unknown precision mode");

@@ -16,6 +16,7 @@ std::unordered_map<const TreeHODLR *, std::shared_ptr<DeviceTree>> g_registry;
 DeviceTree::~DeviceTree() {
   plans.clear();
   mixed.reset();
+  transposed.reset();
   if (arena) cudaFree(arena);
   if (d_leaves) cudaFree(d_leaves);
   if (d_blocks) cudaFree(d_blocks);

@@ -29,6 +29,7 @@ struct DeviceTree {
   std::map<std::tuple<int, int, long long, long long, int, int>, std::unique_ptr<ProductPlan>> plans;
   std::mutex plan_mutex;
   std::shared_ptr<MixedState> mixed;   // int8 slices of the factors (mixed precision)
+  std::shared_ptr<DeviceTree> transposed;   // H^T with the same geometry (mixed op T / L)
   int *mv_woff = nullptr;              // single-vector product: W offset of every block
   double *mv_w = nullptr;              // and W (made on the first such product)
 

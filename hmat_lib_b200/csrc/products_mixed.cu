@@ -1,4 +1,5 @@
-// Mixed-precision HODLR x dense product (op N) on the int8 tensor cores.
+// Mixed-precision HODLR x dense products on the int8 tensor cores: op N
+// directly, op T and op L through the transposed tree (product_mixed_op).
 //
 // The FP64 product's two phases (products.cu), each one launch of the
 // sliced int8 kernel (ozaki.cu):
@@ -19,6 +20,7 @@
 #include <algorithm>
 #include <tuple>
 
+#include "jacobi.h"
 #include "ozaki.h"
 #include "products.h"
 
@@ -455,6 +457,111 @@ void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double 
   ozaki_gemm(P.seg2, P.tile2, P.start2, P.grid2, Y, P.status, s);
   timer.kernel(2, true);
   timer.mark(2);
+}
+
+// ---- H^T X and X H -------------------------------------------------------------------
+
+namespace {
+
+constexpr int kTT = 32;   // transpose tile
+
+// dst (cols x rows, ld ldd) = src^T, src rows x cols (ld lds); 32 x 32 tiles
+// through shared memory (one padding column against bank conflicts).
+__global__ void transpose_kernel(const double *__restrict__ src, long long lds, int rows, int cols,
+                                 double *__restrict__ dst, long long ldd) {
+  __shared__ double tile[kTT][kTT + 1];
+  const int r0 = blockIdx.x * kTT, c0 = blockIdx.y * kTT;
+  const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8 threads
+  for (int j = ty; j < kTT; j += 8) {
+    const int r = r0 + tx, c = c0 + j;
+    if (r < rows && c < cols) tile[j][tx] = src[r + (long long)c * lds];
+  }
+  __syncthreads();
+  for (int j = ty; j < kTT; j += 8) {
+    const int c = c0 + tx, r = r0 + j;   // dst element (c, r)
+    if (r < rows && c < cols) dst[c + (long long)r * ldd] = tile[tx][j];
+  }
+}
+
+void transpose(const double *src, long long lds, int rows, int cols, double *dst, long long ldd,
+               cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  for (int c0 = 0; c0 < cols; c0 += 65535 * kTT) {
+    const int cc = std::min(cols - c0, 65535 * kTT);
+    dim3 grid((rows + kTT - 1) / kTT, (cc + kTT - 1) / kTT);
+    transpose_kernel<<<grid, dim3(kTT, 8), 0, s>>>(src + (long long)c0 * lds, lds, rows, cc,
+                                                  dst + c0, ldd);
+    HB_LAUNCHED();
+  }
+}
+
+// H^T as a device tree of the same geometry: leaf i is D_i^T, block (d, j, c)
+// is the transpose of block (d, j, 3 - c) (U and V swapped), so H^T X is an
+// op-N product of this tree.
+DeviceTree &transposed_tree(DeviceTree &t, cudaStream_t s) {
+  if (t.transposed) return *t.transposed;
+  Geometry gt = t.g;
+  for (int b = 0; b < gt.nblock(); ++b) {
+    const BlockDesc &o = t.g.blocks[b ^ 1];
+    BlockDesc &B = gt.blocks[b];
+    B.m = o.n;
+    B.n = o.m;
+    B.s = o.s;
+  }
+  std::shared_ptr<DeviceTree> tt = dtree_create(gt, s);
+  for (int i = 0; i < gt.nleaf(); ++i) {
+    const int m = t.leaves[i].m;
+    transpose(t.arena + t.leaves[i].off, m, m, m, tt->arena + tt->leaves[i].off, m, s);
+  }
+  std::vector<CopyDesc> cp;
+  for (int b = 0; b < gt.nblock(); ++b) {
+    const BlockDesc &o = t.g.blocks[b ^ 1], &B = tt->g.blocks[b];
+    if (B.s == 0) continue;
+    cp.push_back(CopyDesc{t.arena + o.v_off, o.n, tt->arena + B.u_off, B.m, B.m, B.s});
+    cp.push_back(CopyDesc{t.arena + o.u_off, o.m, tt->arena + B.v_off, B.n, B.n, B.s});
+  }
+  if (!cp.empty()) {
+    CopyDesc *d = upload(cp, s);
+    copy2d_batched(d, (int)cp.size(), s);
+    HB_CUDA(cudaStreamSynchronize(s));
+    cudaFree(d);
+  }
+  t.transposed = tt;
+  return *tt;
+}
+
+}  // namespace
+
+void product_mixed_op(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
+                      long long ldy, cudaStream_t s) {
+  if (op == ProdOp::N) {
+    product_mixed(t, X, k, ldx, Y, ldy, s);
+    return;
+  }
+  if (k <= 0 || t.g.n == 0) return;
+  DeviceTree *tt;
+  {
+    std::lock_guard<std::mutex> lk(t.plan_mutex);
+    tt = &transposed_tree(t, s);
+  }
+  if (op == ProdOp::T) {
+    product_mixed(*tt, X, k, ldx, Y, ldy, s);
+    return;
+  }
+  // X H with X k x n (ld ldx): (X H)^T = H^T X^T
+  const int n = t.g.n;
+  HB_REQUIRE(ldx >= k && ldy >= k, INPUT_ERROR, "leading dimension below k");
+  double *xt = dev_alloc(2 * (size_t)n * k, s);
+  double *yt = xt + (size_t)n * k;
+  transpose(X, ldx, k, n, xt, n, s);
+  try {
+    product_mixed(*tt, xt, k, n, yt, n, s);
+  } catch (...) {
+    dev_free(xt, s);
+    throw;
+  }
+  transpose(yt, n, n, k, Y, ldy, s);
+  dev_free(xt, s);
 }
 
 // ---- many trees, one launch per step -------------------------------------------------

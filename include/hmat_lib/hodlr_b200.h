@@ -45,8 +45,9 @@ const char *hodlr_b200_version(void);
 const char *hodlr_b200_last_error(void);
 /* Runtime knobs (process-wide; read when a call or a cached plan is made).
  * Returns SUCCESS.  Every option the library reads, with its default:
- *   matmat_precision (0): 1 = host-buffer H X (multiply_hodlr_dense) on the
- *       int8 tensor-core path
+ *   matmat_precision (0): 1 = host-buffer products (multiply_hodlr_dense,
+ *       multiply_hodlr_transpose_dense, multiply_dense_hodlr) on the int8
+ *       tensor-core path
  *   host_chunks (0): column chunks of host-buffer products; 0 automatic (up to
  *       4 from 128 columns), 1 one piece, n that many
  *   matvec_kernels (1): one right-hand side by the dedicated matvec kernels;
