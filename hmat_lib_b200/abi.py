@@ -143,6 +143,9 @@ B200_API = {
     "hodlr_b200_matvec_noalloc_dev": (C.c_int, [VP, VP, VP, VP]),
     "hodlr_b200_kernel_matrix_dev": (
         C.c_int, [VP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, VP, C.c_int, VP]),
+    "hodlr_b200_kernel_block_dev": (
+        C.c_int, [VP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                  C.c_int, C.c_int, VP, C.c_int, VP]),
     "hodlr_b200_matmat_batched_dev": (
         C.c_int, [C.c_int, C.POINTER(VP), C.c_int, C.c_int, C.POINTER(VP), IP, IP,
                   C.POINTER(VP), IP, VP]),

@@ -161,6 +161,13 @@ int hodlr_b200_recompress_dev(int m, int n, int s, const double *d_u, int ldu, c
  * 2: exp(-r / l). */
 int hodlr_b200_kernel_matrix_dev(const double *d_points, int n, int dim, int kind, double length,
                                  double diag, double *d_out, int ld, void *stream);
+/* The rows x cols block of that kernel matrix whose first entry is (r0, c0)
+ * (0 <= r0, r0 + rows <= n, likewise for columns), column-major with leading
+ * dimension ld >= rows: for products with kernel matrices too large to hold
+ * whole.  No counterpart in hmat_lib. */
+int hodlr_b200_kernel_block_dev(const double *d_points, int n, int dim, int kind, double length,
+                                double diag, int r0, int c0, int rows, int cols, double *d_out,
+                                int ld, void *stream);
 /* Device time (ms) of the two product phases accumulated since the last call
  * while option "record_phase_times" is non-zero: out[0] projections
  * (W = V^T X), out[1] output bands (Y = D X + sum U W), out[2] number of

@@ -109,3 +109,33 @@ def test_matrix_free_argument_errors():
     with pytest.raises(HodlrError) as e:     # leaf sizes that do not add up
         DeviceTree.build_kernel(d_pts.data_ptr(), 256, 2, 1, 0.1, 1e-2, 1, 1e-8, ms=[100, 100])
     assert e.value.code == abi.INPUT_ERROR
+
+
+def test_kernel_block_matches_full_matrix():
+    """hodlr_b200_kernel_block_dev gives exactly the block of the full kernel
+    matrix at its origin (padded leading dimension, diagonal crossing the
+    block), and rejects blocks that leave the matrix."""
+    import ctypes as C
+
+    import torch
+
+    from hmat_lib_b200 import abi
+    lib = abi.load()
+    n = 700
+    pts = W.points_morton(n, 3, seed=9)
+    d_pts = torch.from_numpy(np.asfortranarray(pts).T.copy().reshape(-1)).cuda()
+    full = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    assert lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, 3, 2, 0.15, 1e-2,
+                                            C.c_void_p(full.data_ptr()), n, None) == 0
+    r0, c0, rows, cols, ld = 100, 90, 250, 333, 260
+    blk = torch.full((cols, ld), float("nan"), dtype=torch.float64, device="cuda")
+    assert lib.hodlr_b200_kernel_block_dev(C.c_void_p(d_pts.data_ptr()), n, 3, 2, 0.15, 1e-2,
+                                           r0, c0, rows, cols, C.c_void_p(blk.data_ptr()), ld,
+                                           None) == 0
+    torch.cuda.synchronize()
+    a = full.view(n, n).cpu().numpy().T                    # column-major -> numpy
+    b = blk.cpu().numpy().T[:rows]
+    assert np.array_equal(b, a[r0:r0 + rows, c0:c0 + cols])
+    assert lib.hodlr_b200_kernel_block_dev(C.c_void_p(d_pts.data_ptr()), n, 3, 2, 0.15, 1e-2,
+                                           n - 10, 0, 11, 5, C.c_void_p(blk.data_ptr()), ld,
+                                           None) == abi.INPUT_ERROR
