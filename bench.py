@@ -49,6 +49,8 @@ def parse():
                     help="skip the n = 1024 H x and n = 16384 H x H measurements")
     ap.add_argument("--batch", type=int, default=512,
                     help="instances of the uneven-batch measurement (0: skip)")
+    ap.add_argument("--no-exp3d", action="store_true",
+                    help="skip the n = 65536 3D exponential (learned-rank) workload")
     return ap.parse_args()
 
 
@@ -285,6 +287,119 @@ def side_workloads(lib, torch, dev, stream, sh):
         ta.free()
         tb.free()
         del da, db
+    torch.cuda.empty_cache()
+    return out
+
+
+def exp3d_workload(lib, torch, dev, stream, steps, warmup):
+    """The learned-rank workload: n = 65536 points of [0,1]^3 (seed 4) in
+    Morton order, exp(-r / 0.15) + 1e-2 I, depth 9 (leaf 128), tol 1e-8,
+    k = 128 right-hand sides.  Both trees are built from the points
+    (matrix-free: the 34 GB matrix is never formed), first by the plain
+    adaptive range finder, then with sketches sized by the shipped rank model
+    (fallback to adaptive growth per block).  Then H X in FP64 and in mixed
+    precision, device-resident, and the error of both trees' products
+    against the dense FP64 product on 16 of the 128 columns, with the kernel
+    matrix generated on the device one block of rows at a time."""
+    import numpy as np
+
+    from hmat_lib_b200 import rank_model as RM
+    from hmat_lib_b200 import workloads as W
+    from hmat_lib_b200.hodlr import DeviceTree
+    w = W.WORKLOADS["exp3d_n65536"]
+    n, h, tol, k = w["n"], w["height"], w["tol"], w["k"]
+    sh = stream.cuda_stream
+    pts = W.workload_points("exp3d_n65536")
+    d_pts = torch.from_numpy(np.asfortranarray(pts).T.copy().reshape(-1)).to(dev)
+    out = {"n": n, "height": h, "tol": tol, "k": k,
+           "kernel": "exp(-r/0.15) + 1e-2 I, 3D Morton points seed 4",
+           "input": "points only (hodlr_b200_build_kernel_dev)"}
+
+    def build(learned):
+        lib.hodlr_b200_set_option(b"learned_ranks", 1.0 if learned else 0.0)
+        try:
+            with torch.cuda.stream(stream):
+                stream.synchronize()
+                torch.cuda.nvtx.range_push("build_exp3d_learned" if learned else "build_exp3d")
+                t0 = time.perf_counter()
+                t = DeviceTree.build_kernel(d_pts.data_ptr(), n, 3, 2, w["length"], w["diag"], h,
+                                            tol, stream=sh)
+                stream.synchronize()
+                sec = time.perf_counter() - t0
+                torch.cuda.nvtx.range_pop()
+        finally:
+            lib.hodlr_b200_set_option(b"learned_ranks", 0.0)
+        return t, sec, build_stats(lib)
+
+    RM.load_default()
+    tree, plain_s, plain_st = build(False)
+    tree_l, learned_s, learned_st = build(True)
+    ranks, ranks_l = tree.ranks(), tree_l.ranks()
+    info = tree.info()
+
+    def by_depth(r):
+        return [int(max(r[2 * ((1 << d) - 1):2 * ((1 << (d + 1)) - 1)])) for d in range(h)]
+
+    x = torch.randn(k, n, dtype=torch.float64, device=dev)        # column-major n x k
+    y = torch.zeros_like(x)
+    bytes_step = 8.0 * info["storage"] + 16.0 * n * k
+    flops_step = 2.0 * k * info["storage"]
+
+    def timed(t, precision):
+        for _ in range(max(3, warmup)):
+            t.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh, precision=precision)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(10, steps)
+        e0.record(stream)
+        for _ in range(reps):
+            t.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh, precision=precision)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        return {"ms_per_step": ms, "GB/s": bytes_step / (ms * 1e-3) / 1e9,
+                "GFLOP/s": flops_step / (ms * 1e-3) / 1e9}
+
+    r64 = timed(tree, 0)
+    rmx = timed(tree, 1)
+    assert lib.hodlr_b200_check(tree.h, C.c_void_p(sh)) == 0, lib.hodlr_b200_last_error()
+    # dense product on 16 columns: (A X)[:, :16], A generated 2048 columns at
+    # a time (A is symmetric, so a column block is the transposed row block)
+    cols, rb = 16, 2048
+    xs = x[:cols].contiguous()                      # row c = column c of X
+    yd = torch.zeros(cols, n, dtype=torch.float64, device=dev)
+    a_blk = torch.empty(n * rb, dtype=torch.float64, device=dev)
+    with torch.cuda.stream(stream):
+        for r0 in range(0, n, rb):
+            assert lib.hodlr_b200_kernel_block_dev(C.c_void_p(d_pts.data_ptr()), n, 3, 2,
+                                                   w["length"], w["diag"], 0, r0, n, rb,
+                                                   C.c_void_p(a_blk.data_ptr()), n,
+                                                   C.c_void_p(sh)) == 0
+            blk = a_blk.view(rb, n)                 # blk[j, i] = A[i, r0 + j]
+            yd[:, r0:r0 + rb] = xs @ blk.t()        # (A X)[r0 + j, c]
+        stream.synchronize()
+    del a_blk
+    errs = {}
+    for name, (t, prec) in (("plain_fp64", (tree, 0)), ("plain_mixed", (tree, 1)),
+                            ("learned_fp64", (tree_l, 0)), ("learned_mixed", (tree_l, 1))):
+        yy = torch.zeros(k, n, dtype=torch.float64, device=dev)
+        t.matmat(x.data_ptr(), k, n, yy.data_ptr(), n, stream=sh, precision=prec)
+        stream.synchronize()
+        errs[name] = (torch.linalg.norm(yy[:cols] - yd) / torch.linalg.norm(yd)).item()
+    out.update({
+        "build": {"plain": dict(seconds=plain_s, **plain_st),
+                  "learned": dict(seconds=learned_s, **learned_st,
+                                  max_rank_diff_vs_plain=int(np.max(np.abs(ranks_l - ranks)))),
+                  "speedup_learned_vs_plain": plain_s / learned_s},
+        "ranks_by_depth": by_depth(ranks), "ranks_by_depth_learned": by_depth(ranks_l),
+        "factor_bytes": 8 * info["storage"], "max_rank": info["max_rank"],
+        "matmat": {"fp64": r64, "mixed": rmx, "bytes_per_step": bytes_step,
+                   "speedup_mixed_vs_fp64": r64["ms_per_step"] / rmx["ms_per_step"]},
+        "rel_err_vs_dense": errs,
+        "check": "H X vs A X on 16 of the 128 columns, A generated on the device"})
+    tree.free()
+    tree_l.free()
+    del x, y, yd
     torch.cuda.empty_cache()
     return out
 
@@ -667,6 +782,10 @@ def main():
     e2e_s = e2e_time(1)
     e2e = bytes_step * world / e2e_s / 1e9
 
+    exp3d = None
+    if not args.no_exp3d:
+        exp3d = exp3d_workload(lib, torch, dev, stream, args.steps, args.warmup)
+
     batch = None
     if args.batch > 0:
         batch = uneven_batch_bench(args.batch, args.steps, args.warmup, lib, torch, dev, stream,
@@ -806,6 +925,7 @@ def main():
         "gpu_launches": rmx["launches"],
         "cpu_baseline": cpu,
         "batch": batch,
+        "exp3d_n65536": exp3d,
     }
     print(json.dumps(line))
     host_tree.free()
