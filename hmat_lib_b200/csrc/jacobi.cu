@@ -147,6 +147,7 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
     theta = 1e-3 * prm.tol * sqrt(f2) / C;
   else if (prm.trunc == Truncation::Absolute)
     theta = 1e-3 * prm.tol / sqrt((double)C);
+  theta = fmax(theta, P.skip_abs);
   const double skip2 = theta * theta;
 
   // a computed dot product of length R carries ~sqrt(R) eps relative noise:

@@ -26,6 +26,8 @@ struct JacobiProb {
   int *sweeps;      // out (optional): sweeps used; max_sweeps + 1 if not converged
   int gen_r0 = -1;  // >= 0: A is the block of the launch's kernel matrix with origin
   int gen_c0 = 0;   //   (gen_r0, gen_c0) (element (i, j) computed, A / lda unused)
+  double skip_abs = 0.0;   // pairs with a column norm at or below this are neither
+                           // rotated nor tested (on top of the truncation's own rule)
 };
 
 enum class Truncation : int {
