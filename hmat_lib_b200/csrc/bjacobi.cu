@@ -1,0 +1,332 @@
+// Block one-sided Jacobi SVD (see bjacobi.h).
+//
+// Per problem, one workspace holds X (the columns being orthogonalised,
+// L x Lp, Lp = L rounded up to whole 16-column blocks, padding columns zero),
+// V (the accumulated right rotations, Lp x Lp), and per pair of blocks a
+// 32-column panel, a copy of the pair's V columns, R, the Jacobi workspace
+// and its outputs.  A round, for every problem at once:
+//   1. copy the pair's X columns into its panel and its V columns aside;
+//   2. TSQR of every panel: panel = Q R (Q written over the panel);
+//   3. one-sided Jacobi SVD of every R: R = (U_R Sigma) W^T, sorted;
+//   4. X[:, pair] = Q (U_R Sigma), V[:, pair] = V_old[:, pair] W (batched GEMMs);
+//   5. a pair whose Jacobi rotated anything marks its problem.
+// Round r of a sweep pairs blocks as the round-robin tournament does (block
+// players - 1 fixed, the others rotating), so a sweep of players - 1 rounds
+// pairs every block with every other once.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "bjacobi.h"
+#include "dtree.h"
+#include "gemm_f64.h"
+#include "jacobi.h"
+#include "tsqr.h"
+
+namespace hb {
+
+namespace {
+
+constexpr int kBj = 16;          // columns per block
+constexpr int kPair = 2 * kBj;   // columns per pair: one TSQR panel
+constexpr int kT = 32;           // transpose tile
+
+template <class T>
+T *upload_vec(const std::vector<T> &v, cudaStream_t s) {
+  T *d = nullptr;
+  HB_CUDA(cudaMallocAsync((void **)&d, sizeof(T) * std::max<size_t>(v.size(), 1), s));
+  if (!v.empty())
+    HB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+// dst[i + j ldd] = src[j + i lds] for i, j < n (32 x 32 tiles through shared
+// memory, one padding column against bank conflicts)
+__global__ void bj_transpose_kernel(const double *__restrict__ src, long long lds, int n,
+                                    double *__restrict__ dst, long long ldd) {
+  __shared__ double tile[kT][kT + 1];
+  const int i0 = blockIdx.x * kT, j0 = blockIdx.y * kT;
+  const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8 threads
+  // tile[jj][ii] = src[(j0 + ii) + (i0 + jj) lds]: coalesced along ii
+  for (int jj = ty; jj < kT; jj += 8)
+    if (i0 + jj < n && j0 + tx < n) tile[jj][tx] = src[(j0 + tx) + (long long)(i0 + jj) * lds];
+  __syncthreads();
+  // dst[(i0 + ii) + (j0 + jj) ldd] = src[(j0 + jj) + (i0 + ii) lds] = tile[ii][jj]
+  for (int jj = ty; jj < kT; jj += 8)
+    if (i0 + tx < n && j0 + jj < n) dst[(i0 + tx) + (long long)(j0 + jj) * ldd] = tile[tx][jj];
+}
+
+__global__ void bj_identity_kernel(double *__restrict__ v, long long ld, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v[i + (long long)i * ld] = 1.0;
+}
+
+// problem owner[k] rotated something in this round when pair slot k's Jacobi
+// needed more than its first (checking) sweep
+__global__ void bj_flag_kernel(const int *__restrict__ sweeps, const int *__restrict__ owner,
+                               int nslots, int *__restrict__ rotated) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nslots; k += gridDim.x * blockDim.x)
+    if (sweeps[k] > 1) rotated[owner[k]] = 1;
+}
+
+// Blocks (a, b) of pair k in round r of a round-robin over `players` (even).
+void round_pair(int k, int r, int players, int &a, int &b) {
+  if (k == 0) {
+    a = r;
+    b = players - 1;
+  } else {
+    a = (r + k) % (players - 1);
+    b = (r - k + (players - 1)) % (players - 1);
+  }
+  if (a > b) std::swap(a, b);
+}
+
+struct Work {
+  int L = 0, Lp = 0, nblk = 0, players = 0, npairs = 0;
+  long long x = 0, v = 0, pnl = 0, tmp = 0, r = 0, jw = 0, ju = 0, jv = 0, js = 0;
+  int slot0 = 0;          // first pair slot of this problem
+  int round = 0, sweep = 0;
+  bool active = true, converged = false;
+  double theta = 0.0;     // column norms at or below this are not rotated
+};
+
+}  // namespace
+
+void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_sweeps,
+                      int *d_status, cudaStream_t s) {
+  const int np = (int)probs.size();
+  if (np == 0) return;
+  // ---- layout ------------------------------------------------------------------------
+  std::vector<Work> wk(np);
+  long long total = 0;
+  auto take = [&](long long e) {
+    const long long o = total;
+    total += align_up(std::max<long long>(e, 1));
+    return o;
+  };
+  const long long jws = jacobi_workspace(kPair, kPair);
+  int nslots = 0, lmax = 0;
+  for (int p = 0; p < np; ++p) {
+    Work &W = wk[p];
+    W.L = probs[p].L;
+    HB_REQUIRE(W.L >= kPair, INPUT_ERROR, "block Jacobi SVD: problem narrower than 32 columns");
+    W.Lp = (W.L + kBj - 1) / kBj * kBj;
+    W.nblk = W.Lp / kBj;
+    W.players = W.nblk + (W.nblk & 1);
+    W.npairs = W.players / 2;
+    W.x = take((long long)W.L * W.Lp);
+    W.v = take((long long)W.Lp * W.Lp);
+    W.pnl = take((long long)W.npairs * W.L * kPair);
+    W.tmp = take((long long)W.npairs * W.Lp * kPair);
+    W.r = take((long long)W.npairs * kPair * kPair);
+    W.jw = take((long long)W.npairs * jws);
+    W.ju = take((long long)W.npairs * kPair * kPair);
+    W.jv = take((long long)W.npairs * kPair * kPair);
+    W.js = take((long long)W.npairs * kPair);
+    W.slot0 = nslots;
+    nslots += W.npairs;
+    lmax = std::max(lmax, W.L);
+  }
+  std::vector<long long> noff(np);   // squared column norms of X
+  for (int p = 0; p < np; ++p) noff[p] = take(wk[p].Lp);
+  double *w = dev_alloc(total, s);
+  HB_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * total, s));
+  int *d_ints = nullptr;   // per slot: rank, sweeps, owner; per problem: rotated flag
+  HB_CUDA(cudaMallocAsync((void **)&d_ints, sizeof(int) * (3 * nslots + np), s));
+  HB_CUDA(cudaMemsetAsync(d_ints, 0, sizeof(int) * (3 * nslots + np), s));
+  int *d_rank = d_ints, *d_sw = d_ints + nslots, *d_owner = d_ints + 2 * nslots;
+  int *d_rot = d_ints + 3 * nslots;
+  {
+    std::vector<int> owner(nslots);
+    for (int p = 0; p < np; ++p)
+      for (int k = 0; k < wk[p].npairs; ++k) owner[wk[p].slot0 + k] = p;
+    HB_CUDA(cudaMemcpyAsync(d_owner, owner.data(), sizeof(int) * nslots, cudaMemcpyHostToDevice,
+                            s));
+  }
+  // ---- X = A^T, V = I, thresholds -------------------------------------------------------
+  std::vector<NormDesc> nd;
+  for (int p = 0; p < np; ++p) {
+    const Work &W = wk[p];
+    dim3 grid((W.L + kT - 1) / kT, (W.L + kT - 1) / kT);
+    bj_transpose_kernel<<<grid, dim3(kT, 8), 0, s>>>(probs[p].A, probs[p].lda, W.L, w + W.x, W.L);
+    HB_LAUNCHED();
+    bj_identity_kernel<<<(W.Lp + 255) / 256, 256, 0, s>>>(w + W.v, W.Lp, W.Lp);
+    HB_LAUNCHED();
+    nd.push_back(NormDesc{w + W.x, W.L, W.L, W.Lp, w + noff[p]});
+  }
+  column_norms2(nd, s);
+  {
+    std::vector<double> h;
+    for (int p = 0; p < np; ++p) {
+      h.resize(wk[p].Lp);
+      HB_CUDA(cudaMemcpyAsync(h.data(), w + noff[p], sizeof(double) * wk[p].Lp,
+                              cudaMemcpyDeviceToHost, s));
+      HB_CUDA(cudaStreamSynchronize(s));
+      double f2 = 0.0;
+      for (double v : h) f2 += v;
+      // the scalar solver's skip rule for the relative truncation
+      wk[p].theta = 1e-3 * tol * std::sqrt(f2) / wk[p].L;
+    }
+  }
+  GemmBases bases{};
+  for (int i = 0; i < kGemmBases; ++i) bases.p[i] = w;
+  JacobiParams prm;
+  prm.trunc = Truncation::None;
+  prm.scale_u = 1;
+  prm.max_sweeps = 60;
+  // a recomputed column pair of length L is orthogonal to about sqrt(L) eps
+  prm.conv_tol = 8.0 * std::sqrt((double)lmax) * 2.220446049250313e-16;
+  std::vector<int> rot(np, 0);
+
+  // ---- rounds ------------------------------------------------------------------------------
+  for (long long guard = 0; guard < 1000000; ++guard) {
+    bool any = false;
+    for (const Work &W : wk) any = any || W.active;
+    if (!any) break;
+    std::vector<CopyDesc> cp;
+    std::vector<TsqrProb> tq;
+    std::vector<JacobiProb> jp;
+    GemmBatch gx, gv;
+    HB_CUDA(cudaMemsetAsync(d_sw, 0, sizeof(int) * nslots, s));
+    for (int p = 0; p < np; ++p) {
+      const Work &W = wk[p];
+      if (!W.active) continue;
+      const long long L = W.L, Lp = W.Lp;
+      for (int k = 0; k < W.npairs; ++k) {
+        int a, b;
+        round_pair(k, W.round, W.players, a, b);
+        if (b >= W.nblk) continue;   // the bye of an odd block count
+        const long long pk = W.pnl + (long long)k * L * kPair;
+        const long long tk = W.tmp + (long long)k * Lp * kPair;
+        const long long rk = W.r + (long long)k * kPair * kPair;
+        const long long uk = W.ju + (long long)k * kPair * kPair;
+        const long long vk = W.jv + (long long)k * kPair * kPair;
+        const long long xa = W.x + (long long)a * kBj * L, xb = W.x + (long long)b * kBj * L;
+        const long long va = W.v + (long long)a * kBj * Lp, vb = W.v + (long long)b * kBj * Lp;
+        cp.push_back(CopyDesc{w + xa, L, w + pk, L, (int)L, kBj});
+        cp.push_back(CopyDesc{w + xb, L, w + pk + kBj * L, L, (int)L, kBj});
+        cp.push_back(CopyDesc{w + va, Lp, w + tk, Lp, (int)Lp, kBj});
+        cp.push_back(CopyDesc{w + vb, Lp, w + tk + kBj * Lp, Lp, (int)Lp, kBj});
+        tq.push_back(TsqrProb{w + pk, L, (int)L, kPair, w + rk, kPair});
+        JacobiProb j{};
+        j.A = w + rk;
+        j.lda = kPair;
+        j.transA = 0;
+        j.m = kPair;
+        j.n = kPair;
+        j.G = w + W.jw + (long long)k * jws;
+        j.W = j.G + align_up((long long)kPair * kPair);
+        j.U = w + uk;
+        j.ldu = kPair;
+        j.V = w + vk;
+        j.ldv = kPair;
+        j.sigma = w + W.js + (long long)k * kPair;
+        j.rank = d_rank + W.slot0 + k;
+        j.sweeps = d_sw + W.slot0 + k;
+        j.skip_abs = W.theta;
+        jp.push_back(j);
+        // X[:, a] = Q (U_R S)[:, 0:16], X[:, b] = Q (U_R S)[:, 16:32]
+        int q = gx.add(0, xa, L, (int)L, kBj);
+        gx.seg(q, 0, pk, L, 0, 0, uk, kPair, 0, kPair);
+        q = gx.add(0, xb, L, (int)L, kBj);
+        gx.seg(q, 0, pk, L, 0, 0, uk + kBj * kPair, kPair, 0, kPair);
+        // V[:, a] = V_old[:, pair] W[:, 0:16], V[:, b] = V_old[:, pair] W[:, 16:32]
+        q = gv.add(0, va, Lp, (int)Lp, kBj);
+        gv.seg(q, 0, tk, Lp, 0, 0, vk, kPair, 0, kPair);
+        q = gv.add(0, vb, Lp, (int)Lp, kBj);
+        gv.seg(q, 0, tk, Lp, 0, 0, vk + kBj * kPair, kPair, 0, kPair);
+      }
+    }
+    if (!cp.empty()) {
+      CopyDesc *d = upload_vec(cp, s);
+      copy2d_batched(d, (int)cp.size(), s);
+      cudaFreeAsync(d, s);
+      tsqr_batched(tq, s);
+      JacobiProb *dj = upload_vec(jp, s);
+      jacobi_svd_batched(dj, (int)jp.size(), prm, d_status, kPair, s);
+      cudaFreeAsync(dj, s);
+      gemm_f64_run(gx, bases, TileShape::M128N64, s, false);
+      gemm_f64_run(gv, bases, TileShape::M128N64, s, false);
+      bj_flag_kernel<<<(nslots + 255) / 256, 256, 0, s>>>(d_sw, d_owner, nslots, d_rot);
+      HB_LAUNCHED();
+    }
+    // end of a sweep: a problem whose sweep rotated nothing has converged
+    bool check = false;
+    for (Work &W : wk) {
+      if (!W.active) continue;
+      if (++W.round == W.players - 1) check = true;
+    }
+    if (!check) continue;
+    HB_CUDA(cudaMemcpyAsync(rot.data(), d_rot, sizeof(int) * np, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    for (int p = 0; p < np; ++p) {
+      Work &W = wk[p];
+      if (!W.active || W.round != W.players - 1) continue;
+      W.round = 0;
+      ++W.sweep;
+      if (!rot[p]) {
+        W.active = false;
+        W.converged = true;
+      } else if (W.sweep >= max_sweeps) {
+        W.active = false;
+      } else {
+        HB_CUDA(cudaMemsetAsync(d_rot + p, 0, sizeof(int), s));
+      }
+    }
+  }
+
+  // ---- singular values, order, rank, outputs -------------------------------------------
+  nd.clear();
+  for (int p = 0; p < np; ++p) nd.push_back(NormDesc{w + wk[p].x, wk[p].L, wk[p].L, wk[p].Lp,
+                                                     w + noff[p]});
+  column_norms2(nd, s);
+  std::vector<CopyDesc> gather;
+  std::vector<std::vector<double>> sig(np);
+  std::vector<int> ranks(np), sweeps(np);
+  for (int p = 0; p < np; ++p) {
+    const Work &W = wk[p];
+    std::vector<double> n2(W.Lp);
+    HB_CUDA(cudaMemcpyAsync(n2.data(), w + noff[p], sizeof(double) * W.Lp,
+                            cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> perm(W.Lp);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return n2[a] > n2[b]; });
+    sig[p].resize(W.L);
+    for (int c = 0; c < W.L; ++c) sig[p][c] = std::sqrt(std::max(n2[perm[c]], 0.0));
+    const double s0 = sig[p][0];
+    int r = 1;
+    if (s0 > tol)
+      while (r < W.L && sig[p][r] >= tol * s0) ++r;
+    ranks[p] = r;
+    sweeps[p] = W.converged ? W.sweep : max_sweeps + 1;
+    for (int c = 0; c < W.L; ++c) {
+      gather.push_back(CopyDesc{w + W.x + (long long)perm[c] * W.L, W.L,
+                                probs[p].U + (long long)c * W.L, W.L, W.L, 1});
+      gather.push_back(CopyDesc{w + W.v + (long long)perm[c] * W.Lp, W.Lp,
+                                probs[p].V + (long long)c * W.L, W.L, W.L, 1});
+    }
+  }
+  CopyDesc *dg = upload_vec(gather, s);
+  copy2d_batched(dg, (int)gather.size(), s);
+  cudaFreeAsync(dg, s);
+  bool failed = false;
+  for (int p = 0; p < np; ++p) {
+    HB_CUDA(cudaMemcpyAsync(probs[p].sigma, sig[p].data(), sizeof(double) * wk[p].L,
+                            cudaMemcpyHostToDevice, s));
+    HB_CUDA(cudaMemcpyAsync(probs[p].rank, &ranks[p], sizeof(int), cudaMemcpyHostToDevice, s));
+    if (probs[p].sweeps)
+      HB_CUDA(cudaMemcpyAsync(probs[p].sweeps, &sweeps[p], sizeof(int), cudaMemcpyHostToDevice,
+                              s));
+    failed = failed || !wk[p].converged;
+  }
+  if (failed) {
+    const int st = SVD_FAILURE;
+    HB_CUDA(cudaMemcpyAsync(d_status, &st, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  HB_CUDA(cudaStreamSynchronize(s));
+  cudaFreeAsync(d_ints, s);
+  dev_free(w, s);
+}
+
+}  // namespace hb

@@ -22,6 +22,7 @@
 #include <chrono>
 #include <cmath>
 
+#include "bjacobi.h"
 #include "build.h"
 #include "jacobi.h"
 #include "rank_mlp.h"
@@ -627,30 +628,39 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   HB_CUDA(cudaEventRecord(ev[2], stream));
 
   // ---- SVD of R_B^T for the sketched blocks ------------------------------------------
+  // Cores of at least jacobi_block_min_c columns go to the block Jacobi solver
+  // (GEMM- and QR-shaped rounds over all SMs); the others to the one-CTA /
+  // one-cluster solver.
+  const int bj_min = (int)option("jacobi_block_min_c", 1024);
   std::vector<JacobiProb> sprobs;
   std::vector<long long> s_u(sk.size()), s_v(sk.size());
   int max_l = 0;
   long long jscratch = 0;
   for (size_t i = 0; i < sk.size(); ++i) {
     const int L = sk[i].ell;
-    max_l = std::max(max_l, L);
-    jscratch += jacobi_workspace(L, L) + 2 * align_up((long long)L * L) + align_up(L);
+    const bool big = L >= bj_min;
+    if (!big) max_l = std::max(max_l, L);
+    jscratch += (big ? 0 : jacobi_workspace(L, L)) + 2 * align_up((long long)L * L) + align_up(L);
   }
   double *jwork = sk.empty() ? nullptr : dev_alloc(jscratch, stream);
+  std::vector<char> is_big(sk.size(), 0);
   {
     long long o = 0;
     for (size_t i = 0; i < sk.size(); ++i) {
       const SketchBlock &S = sk[i];
       const int L = S.ell;
+      is_big[i] = L >= bj_min;
       JacobiProb jp{};
       jp.A = work + S.rb;
       jp.lda = S.cap;
       jp.transA = 1;
       jp.m = L;
       jp.n = L;
-      jp.G = jwork + o;
-      jp.W = jp.G + align_up((long long)L * L);
-      o += jacobi_workspace(L, L);
+      if (!is_big[i]) {
+        jp.G = jwork + o;
+        jp.W = jp.G + align_up((long long)L * L);
+        o += jacobi_workspace(L, L);
+      }
       jp.U = jwork + o;
       s_u[i] = o;
       jp.ldu = L;
@@ -667,9 +677,21 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     }
   }
   JacobiProb *d_sprobs = nullptr;
-  if (!sprobs.empty()) {
-    d_sprobs = upload_vec(sprobs, stream);
-    jacobi_svd_batched(d_sprobs, (int)sprobs.size(), prm, d_status, max_l, stream);
+  {
+    std::vector<JacobiProb> small;
+    std::vector<BjProb> big;
+    for (size_t i = 0; i < sk.size(); ++i) {
+      const JacobiProb &jp = sprobs[i];
+      if (is_big[i])
+        big.push_back(BjProb{jp.A, jp.lda, jp.m, jp.U, jp.V, jp.sigma, jp.rank, jp.sweeps});
+      else
+        small.push_back(jp);
+    }
+    if (!small.empty()) {
+      d_sprobs = upload_vec(small, stream);
+      jacobi_svd_batched(d_sprobs, (int)small.size(), prm, d_status, max_l, stream);
+    }
+    if (!big.empty()) block_jacobi_svd(big, tol, prm.max_sweeps, d_status, stream);
   }
   HB_CUDA(cudaEventRecord(ev[3], stream));
   std::vector<int> ints(2 * n_int, 0);

@@ -79,6 +79,8 @@ const char *hodlr_b200_last_error(void);
  *   jacobi_max_sweeps (60): Jacobi sweep bound (SVD_FAILURE past it)
  *   jacobi_cluster_min_c (192): problems this wide or wider use a cluster of
  *       8 CTAs
+ *   jacobi_block_min_c (1024): sketch cores this wide or wider are solved by
+ *       the block Jacobi SVD (16-column blocks, QR + small SVD + GEMM rounds)
  *   hxh_dense_max (256): H x H blocks up to this many rows are recompressed
  *       from their dense product
  *   autotune (1), batch_shape (-1), use_graphs (1), check_status (0): batched
