@@ -122,6 +122,8 @@ B200_API = {
     "hodlr_b200_build_dev": (
         C.c_int, [C.c_int, C.c_int, IP, VP, C.c_int, C.c_double, C.c_int, VP,
                   C.POINTER(VP), IP]),
+    "hodlr_b200_build_batched_dev": (
+        C.c_int, [C.c_int, IP, IP, C.POINTER(VP), IP, C.c_double, VP, C.POINTER(VP), IP]),
     "hodlr_b200_tree_free": (None, [VP]),
     "hodlr_b200_tree_to_host": (C.c_int, [VP, TP, IP]),
     "hodlr_b200_tree_from_host": (VP, [TP, IP]),

@@ -451,6 +451,36 @@ int hodlr_b200_build_dev(int height, int n, const int *ms, const double *d_matri
   }
 }
 
+int hodlr_b200_build_batched_dev(int count, const int *heights, const int *ns,
+                                 const double *const *d_matrices, const int *lds,
+                                 double svd_threshold, void *stream, hodlr_b200_tree *out,
+                                 int *ierr) {
+  if (count < 0 || (count > 0 && (!heights || !ns || !d_matrices || !lds || !out))) {
+    if (ierr) *ierr = INPUT_ERROR;
+    return INPUT_ERROR;
+  }
+  if (count == 0) {
+    if (ierr) *ierr = SUCCESS;
+    return SUCCESS;
+  }
+  try {
+    std::vector<BuildInput> in;
+    for (int i = 0; i < count; ++i) {
+      HB_REQUIRE(heights[i] >= 1 && ns[i] >= 0 && d_matrices[i] && lds[i] >= std::max(ns[i], 1),
+                 INPUT_ERROR, "batched build: a tree with an invalid height, size or input");
+      Geometry g = geometry_from_leaves(heights[i], halves(ns[i], heights[i]));
+      in.push_back(BuildInput{g, d_matrices[i], lds[i]});
+    }
+    int status = SUCCESS;
+    auto dts = build_batch(in, svd_threshold, as_stream(stream), &status);
+    for (int i = 0; i < count; ++i) out[i] = new hodlr_b200_tree_s{dts[i]};
+    if (ierr) *ierr = status;
+    return status;
+  } catch (const Error &e) {
+    return fail(ierr, e);
+  }
+}
+
 void hodlr_b200_tree_free(hodlr_b200_tree t) { delete t; }
 
 int hodlr_b200_tree_to_host(hodlr_b200_tree t, TreeHODLR *hodlr, int *ierr) {

@@ -45,7 +45,10 @@ T *upload_vec(const std::vector<T> &v, cudaStream_t s) {
 }
 
 struct SketchBlock {
-  int b;                 // block index in the geometry
+  int b;                 // index into the build's flattened block list
+  int bid;               // block index in its own tree (names its random test matrices)
+  int depth;
+  long long lda;         // leading dimension of the block's input
   int m, n, cap;
   long long a_off;       // offset of the block in the input (base kA)
   long long q, bt, p, rb, om, t, c, rn;   // offsets in the work buffer
@@ -68,8 +71,8 @@ constexpr int kFeatCols = 16;   // width of the feature sketch
 // Gaussian sketch Y = A_b Omega, its R factor by TSQR and the singular values
 // of R (= those of Y) by the batched Jacobi SVD, then log block size, depth,
 // ln(kernel length) and five log ratios of the sketch's singular values.
-std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlock> &sk,
-                                  const double *d_A, long long lda, int aslot,
+std::vector<float> block_features(const std::vector<SketchBlock> &sk,
+                                  const double *d_A, int aslot,
                                   const KernelSpec &gen, unsigned long long seed,
                                   cudaStream_t stream) {
   const int nsk = (int)sk.size();
@@ -101,7 +104,7 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
   std::vector<RandDesc> rd;
   for (int i = 0; i < nsk; ++i)
     rd.push_back(RandDesc{w + om[i], sk[i].n, sk[i].n, F,
-                          (1ULL << 60) + ((unsigned long long)sk[i].b << 8)});
+                          (1ULL << 60) + ((unsigned long long)sk[i].bid << 8)});
   gaussian_fill(rd, seed, stream);
   GemmBases bases{};
   bases.p[0] = const_cast<double *>(d_A);
@@ -111,7 +114,7 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
   for (int i = 0; i < nsk; ++i) {
     const SketchBlock &S = sk[i];
     int pr = gb.add(1, y[i], S.m, S.m, F);
-    gb.seg(pr, aslot, S.a_off, lda, 0, 1, om[i], S.n, 0, S.n);
+    gb.seg(pr, aslot, S.a_off, S.lda, 0, 1, om[i], S.n, 0, S.n);
   }
   gemm_f64_run(gb, bases, TileShape::M128N64, stream);
   std::vector<TsqrProb> tp;
@@ -164,7 +167,7 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
     const SketchBlock &S = sk[i];
     float *row = &f[(size_t)i * kRankIn];
     row[0] = (float)std::log2((double)std::min(S.m, S.n));
-    row[1] = (float)g.blocks[S.b].depth;
+    row[1] = (float)S.depth;
     row[2] = length > 0.0 ? (float)std::log(length) : 0.f;
     const double *sv = &sig[(size_t)i * F];
     const int idx[5] = {1, 3, 7, 11, 15};   // s_2, s_4, s_8, s_12, s_16
@@ -180,14 +183,38 @@ std::vector<float> block_features(const Geometry &g, const std::vector<SketchBlo
 const BuildStats &last_build_stats() { return g_last_stats; }
 const std::vector<float> &last_build_features() { return g_last_features; }
 
-std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double *d_A,
-                                             long long lda, double tol, cudaStream_t stream,
-                                             int *svd_status, BuildStats *stats,
-                                             const KernelSpec *gen) {
+std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInput> &in,
+                                                     double tol, cudaStream_t stream,
+                                                     int *svd_status, BuildStats *stats,
+                                                     const KernelSpec *gen) {
   auto t0 = std::chrono::steady_clock::now();
-  Geometry g = g_in;
-  const int nb = g.nblock();
+  HB_REQUIRE(!in.empty(), INPUT_ERROR, "build: no tree to build");
+  HB_REQUIRE(!gen || in.size() == 1, INPUT_ERROR, "a matrix-free build takes one tree");
   *svd_status = SUCCESS;
+  // Every off-diagonal block of every tree, flattened.  The inputs are
+  // addressed as element offsets from the lowest input address, so one GEMM
+  // launch can read blocks of all of them.
+  std::vector<Geometry> gs;
+  const double *d_A = nullptr;
+  for (const BuildInput &x : in) {
+    gs.push_back(x.g);
+    if (x.A && (!d_A || x.A < d_A)) d_A = x.A;
+  }
+  struct Blk {
+    int t, b;
+    BlockDesc B;
+    long long a0;    // first entry of the block: offset from d_A (or generated origin)
+    long long lda;
+  };
+  std::vector<Blk> blk;
+  for (int t = 0; t < (int)in.size(); ++t)
+    for (int b = 0; b < gs[t].nblock(); ++b) {
+      const BlockDesc &B = gs[t].blocks[b];
+      const long long a0 = gen ? gen_offset(B.r0, B.c0)
+                               : (long long)(in[t].A - d_A) + B.r0 + (long long)B.c0 * in[t].lda;
+      blk.push_back(Blk{t, b, B, a0, in[t].lda});
+    }
+  const int nb = (int)blk.size();
   const int exact_max = (int)option("exact_max", 128);
   const int cap_opt = (int)option("sketch_cap", 0.0) / kPanel * kPanel;
   const int w_first = std::max(kPanel, (int)option("sketch_first", 64) / kPanel * kPanel);
@@ -201,7 +228,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   // ---- partition the blocks --------------------------------------------------
   std::vector<int> exact, sketched;
   for (int b = 0; b < nb; ++b) {
-    const BlockDesc &B = g.blocks[b];
+    const BlockDesc &B = blk[b].B;
     const int C = std::min(B.m, B.n);
     if (C == 0) continue;
     (C <= exact_max ? exact : sketched).push_back(b);
@@ -218,7 +245,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   std::vector<ExactSlot> eslots;
   int max_c = 0;
   for (int b : exact) {
-    const BlockDesc &B = g.blocks[b];
+    const BlockDesc &B = blk[b].B;
     const int C = std::min(B.m, B.n);
     ExactSlot s;
     s.ws = take(jacobi_workspace(B.m, B.n));
@@ -247,7 +274,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     auto bytes_of = [&](double alpha) {
       double total = 0.0;
       for (int b : sketched) {
-        const BlockDesc &B = g.blocks[b];
+        const BlockDesc &B = blk[b].B;
         const double c = cap_of(B, alpha);
         // q, bt, p, rb, om, t, c, rn, and the core SVD's G, W, U, V
         total += 8.0 * ((double)B.m * c + 2.0 * B.n * c + c * c + (double)B.n * w_round +
@@ -282,18 +309,21 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
         alpha = lo;
       }
     }
-    for (size_t i = 0; i < sketched.size(); ++i) caps[i] = cap_of(g.blocks[sketched[i]], alpha);
+    for (size_t i = 0; i < sketched.size(); ++i) caps[i] = cap_of(blk[sketched[i]].B, alpha);
   }
   std::vector<SketchBlock> sk;
   for (size_t si = 0; si < sketched.size(); ++si) {
     const int b = sketched[si];
-    const BlockDesc &B = g.blocks[b];
+    const BlockDesc &B = blk[b].B;
     SketchBlock S;
     S.b = b;
+    S.bid = blk[b].b;
+    S.depth = B.depth;
+    S.lda = blk[b].lda;
     S.m = B.m;
     S.n = B.n;
     S.cap = caps[si];
-    S.a_off = gen ? gen_offset(B.r0, B.c0) : B.r0 + (long long)B.c0 * lda;
+    S.a_off = blk[b].a0;
     sk.push_back(S);
   }
   // ---- learned sizing of the first sketch ---------------------------------------------
@@ -305,7 +335,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   for (SketchBlock &S : sk) S.first_w = std::min(w_first, S.cap);
   const auto tf0 = std::chrono::steady_clock::now();
   if (record && !sk.empty()) {
-    feats = block_features(g, sk, d_A, lda, aslot, gspec, seed, stream);
+    feats = block_features(sk, d_A, aslot, gspec, seed, stream);
     if (have_model) {
       const int nsk = (int)sk.size();
       float *dbuf = nullptr;
@@ -384,16 +414,16 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   // ---- exact path ----------------------------------------------------------------
   std::vector<JacobiProb> eprobs;
   for (size_t p = 0; p < exact.size(); ++p) {
-    const BlockDesc &B = g.blocks[exact[p]];
+    const BlockDesc &B = blk[exact[p]].B;
     const int R = std::max(B.m, B.n), C = std::min(B.m, B.n);
     JacobiProb jp{};
     if (gen) {
       jp.gen_r0 = B.r0;
       jp.gen_c0 = B.c0;
     } else {
-      jp.A = d_A + B.r0 + (long long)B.c0 * lda;
+      jp.A = d_A + blk[exact[p]].a0;
     }
-    jp.lda = lda;
+    jp.lda = blk[exact[p]].lda;
     jp.transA = 0;
     jp.m = B.m;
     jp.n = B.n;
@@ -442,7 +472,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     std::vector<RandDesc> rd;
     for (int i : act)
       rd.push_back(RandDesc{work + sk[i].om, sk[i].n, sk[i].n, wb[i],
-                            ((unsigned long long)sk[i].b << 24) + (unsigned long long)rounds});
+                            ((unsigned long long)sk[i].bid << 24) + (unsigned long long)rounds});
     gaussian_fill(rd, seed, stream);
 
     // 2. Y = A Om written into the new columns of Q; 3. Y -= Q (B Om)
@@ -451,7 +481,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
       for (int i : act) {
         const SketchBlock &S = sk[i];
         int pr = g1.add(kWork, S.q + (long long)S.ell * S.m, S.m, S.m, wb[i]);
-        g1.seg(pr, aslot, S.a_off, lda, 0, kWork, S.om, S.n, 0, S.n);
+        g1.seg(pr, aslot, S.a_off, S.lda, 0, kWork, S.om, S.n, 0, S.n);
       }
       gemm_f64_run(g1, bases, TileShape::M128N64, stream);
       // ||A om_c||^2: the scale against which a projected column counts as noise
@@ -568,7 +598,7 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
       for (int i : act) {
         const SketchBlock &S = sk[i];
         int pr = g5.add(kWork, S.bt + (long long)S.ell * S.n, S.n, S.n, wb[i]);
-        g5.seg(pr, aslot, S.a_off, lda, 1, kWork, S.q + (long long)S.ell * S.m, S.m, 0, S.m);
+        g5.seg(pr, aslot, S.a_off, S.lda, 1, kWork, S.q + (long long)S.ell * S.m, S.m, 0, S.m);
       }
       gemm_f64_run(g5, bases, TileShape::M128N64, stream);
       std::vector<CopyDesc> cp;
@@ -724,29 +754,37 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     fro_rank[i] = r;
   }
   *svd_status = ints[n_int - 1];
-  for (auto &B : g.blocks) B.s = 0;
-  for (size_t p = 0; p < exact.size(); ++p) g.blocks[exact[p]].s = ints[p];
-  for (size_t i = 0; i < sk.size(); ++i) g.blocks[sk[i].b].s = ints[exact.size() + i];
+  for (Geometry &g : gs)
+    for (auto &B : g.blocks) B.s = 0;
+  for (size_t p = 0; p < exact.size(); ++p)
+    gs[blk[exact[p]].t].blocks[blk[exact[p]].b].s = ints[p];
+  for (size_t i = 0; i < sk.size(); ++i)
+    gs[blk[sk[i].b].t].blocks[blk[sk[i].b].b].s = ints[exact.size() + i];
 
-  // ---- arena: leaves from the input, factors from the scratch ------------------------
-  std::shared_ptr<DeviceTree> dt = dtree_create(g, stream);
+  // ---- arenas: leaves from the input, factors from the scratch ------------------------
+  std::vector<std::shared_ptr<DeviceTree>> dts;
+  for (const Geometry &g : gs) dts.push_back(dtree_create(g, stream));
   std::vector<CopyDesc> copies;
   std::vector<GenBlock> gen_leaves;
-  for (int i = 0; i < g.nleaf(); ++i) {
-    const LeafDesc &L = dt->leaves[i];
-    if (L.m == 0) continue;
-    if (gen)
-      gen_leaves.push_back(GenBlock{L.r0, L.r0, L.m, L.m, dt->arena + L.off, L.m});
-    else
-      copies.push_back(
-          CopyDesc{d_A + L.r0 + (long long)L.r0 * lda, lda, dt->arena + L.off, L.m, L.m, L.m});
+  for (size_t t = 0; t < dts.size(); ++t) {
+    const DeviceTree &dt = *dts[t];
+    for (int i = 0; i < dt.g.nleaf(); ++i) {
+      const LeafDesc &L = dt.leaves[i];
+      if (L.m == 0) continue;
+      if (gen)
+        gen_leaves.push_back(GenBlock{L.r0, L.r0, L.m, L.m, dt.arena + L.off, L.m});
+      else
+        copies.push_back(CopyDesc{in[t].A + L.r0 + (long long)L.r0 * in[t].lda, in[t].lda,
+                                  dt.arena + L.off, L.m, L.m, L.m});
+    }
   }
   kernel_blocks(gspec, gen_leaves, stream);
   for (size_t p = 0; p < exact.size(); ++p) {
-    const BlockDesc &B = dt->g.blocks[exact[p]];
+    const DeviceTree &dt = *dts[blk[exact[p]].t];
+    const BlockDesc &B = dt.g.blocks[blk[exact[p]].b];
     if (B.s == 0) continue;
-    copies.push_back(CopyDesc{eprobs[p].U, B.m, dt->arena + B.u_off, B.m, B.m, B.s});
-    copies.push_back(CopyDesc{eprobs[p].V, B.n, dt->arena + B.v_off, B.n, B.n, B.s});
+    copies.push_back(CopyDesc{eprobs[p].U, B.m, dt.arena + B.u_off, B.m, B.m, B.s});
+    copies.push_back(CopyDesc{eprobs[p].V, B.n, dt.arena + B.v_off, B.n, B.n, B.s});
   }
   if (!copies.empty()) {
     CopyDesc *d = upload_vec(copies, stream);
@@ -754,20 +792,25 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
     cudaFreeAsync(d, stream);
   }
   if (!sk.empty()) {
-    // U = Q[:, :ell] (U_R Sigma)[:, :s],  V = P[:, :ell] V_R[:, :s]
+    // U = Q[:, :ell] (U_R Sigma)[:, :s],  V = P[:, :ell] V_R[:, :s]; the arenas
+    // are addressed from the lowest arena address
+    double *abase = dts[0]->arena;
+    for (auto &dt : dts) abase = std::min(abase, dt->arena);
     GemmBases fb{};
     fb.p[0] = work;
     fb.p[1] = jwork;
-    fb.p[2] = dt->arena;
+    fb.p[2] = abase;
     for (int i = 3; i < kGemmBases; ++i) fb.p[i] = work;
     GemmBatch gf;
     for (size_t i = 0; i < sk.size(); ++i) {
       const SketchBlock &S = sk[i];
-      const BlockDesc &B = dt->g.blocks[S.b];
+      const DeviceTree &dt = *dts[blk[S.b].t];
+      const BlockDesc &B = dt.g.blocks[blk[S.b].b];
       if (B.s == 0) continue;
-      int pu = gf.add(2, B.u_off, B.m, B.m, B.s);
+      const long long ao = (long long)(dt.arena - abase);
+      int pu = gf.add(2, ao + B.u_off, B.m, B.m, B.s);
       gf.seg(pu, 0, S.q, S.m, 0, 1, s_u[i], S.ell, 0, S.ell);
-      int pv = gf.add(2, B.v_off, B.n, B.n, B.s);
+      int pv = gf.add(2, ao + B.v_off, B.n, B.n, B.s);
       gf.seg(pv, 0, S.p, S.n, 0, 1, s_v[i], S.ell, 0, S.ell);
     }
     gemm_f64_run(gf, fb, TileShape::M128N64, stream, false);
@@ -828,7 +871,13 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g_in, const double 
   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   g_last_stats = st;
   if (stats) *stats = st;
-  return dt;
+  return dts;
+}
+
+std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g, const double *d_A, long long lda,
+                                             double tol, cudaStream_t stream, int *svd_status,
+                                             BuildStats *stats, const KernelSpec *gen) {
+  return build_batch({BuildInput{g, d_A, lda}}, tol, stream, svd_status, stats, gen)[0];
 }
 
 }  // namespace hb

@@ -49,4 +49,21 @@ std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g, const double *d_
                                              BuildStats *stats = nullptr,
                                              const KernelSpec *gen = nullptr);
 
+// One tree of a batch build: its block sizes and its n x n input (ld lda).
+struct BuildInput {
+  Geometry g;
+  const double *A;
+  long long lda;
+};
+
+// Builds many trees at once: the blocks of every tree share the launches of
+// every stage (exact Jacobi SVDs, sketch rounds, core SVDs, finishing), and
+// each tree gets the same random test matrices, so the same ranks, as when
+// built alone.  `svd_status` is SVD_FAILURE if any tree's build failed.  With
+// `gen` the batch must hold one tree.
+std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInput> &in,
+                                                     double tol, cudaStream_t stream,
+                                                     int *svd_status, BuildStats *stats = nullptr,
+                                                     const KernelSpec *gen = nullptr);
+
 }  // namespace hb

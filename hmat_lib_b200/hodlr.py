@@ -189,6 +189,26 @@ class DeviceTree:
         return cls(out)
 
     @classmethod
+    def build_batched(cls, d_matrix_ptrs, ns, lds, heights, tol: float,
+                      stream: int = 0) -> list:
+        """hodlr_b200_build_batched_dev: many trees in shared launches."""
+        count = len(ns)
+        arr = lambda T, v: (T * max(count, 1))(*v)
+        out = (C.c_void_p * max(count, 1))()
+        ierr = C.c_int(0)
+        lib().hodlr_b200_build_batched_dev(count, arr(C.c_int, heights), arr(C.c_int, ns),
+                                           arr(C.c_void_p, d_matrix_ptrs), arr(C.c_int, lds),
+                                           tol, C.c_void_p(stream), out, C.byref(ierr))
+        trees = [cls(C.c_void_p(out[i])) for i in range(count)] \
+            if ierr.value in (abi.SUCCESS, abi.SVD_FAILURE) else []
+        if ierr.value != abi.SUCCESS:
+            msg = lib().hodlr_b200_last_error().decode()
+            for t in trees:
+                t.free()
+            raise HodlrError(ierr.value, "hodlr_b200_build_batched_dev", msg)
+        return trees
+
+    @classmethod
     def build_kernel(cls, d_points_ptr: int, n: int, dim: int, kind: int, length: float,
                      diag: float, height: int, tol: float, stream: int = 0,
                      ms=None) -> "DeviceTree":

@@ -109,6 +109,19 @@ long long hodlr_b200_kernel_launches(void);
 int hodlr_b200_build_dev(int height, int n, const int *ms, const double *d_matrix, int ld,
                          double svd_threshold, int flags, void *stream, hodlr_b200_tree *out,
                          int *ierr);
+/* Builds `count` trees at once, tree i of height heights[i] from the
+ * ns[i] x ns[i] device matrix d_matrices[i] (leading dimension lds[i], block
+ * sizes halved as dense_to_tree_hodlr does), all with relative tolerance
+ * svd_threshold: the blocks of every tree share the launches of every stage,
+ * and each tree comes out as it would from hodlr_b200_build_dev.  The trees
+ * go to out[0 .. count-1] (free each with hodlr_b200_tree_free); on
+ * SVD_FAILURE (any tree) the trees are still stored, on other errors none.
+ * hmat_lib builds one tree per call (dense_to_tree_hodlr,
+ * src/constructors.c:629). */
+int hodlr_b200_build_batched_dev(int count, const int *heights, const int *ns,
+                                 const double *const *d_matrices, const int *lds,
+                                 double svd_threshold, void *stream, hodlr_b200_tree *out,
+                                 int *ierr);
 void hodlr_b200_tree_free(hodlr_b200_tree t);
 /* Fills an allocated, empty host tree of the same height with copies of the
  * device factors (library allocator; free with free_tree_data). */
