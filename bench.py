@@ -444,6 +444,37 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, r
             ns.append(n)
         del a
     torch.cuda.empty_cache()
+    # the same trees built in batches (hodlr_b200_build_batched_dev): groups of
+    # up to 64 trees, each group's inputs generated first, then one batched
+    # build per group (the timed part); ranks compared with the per-tree builds
+    batched_s, rank_mismatch = 0.0, 0
+    group = 64
+    with torch.cuda.stream(stream):
+        for g0 in range(0, len(inst), group):
+            grp = inst[g0:g0 + group]
+            mats = []
+            for it in grp:
+                n = it["n"]
+                d_pts = torch.from_numpy(np.ascontiguousarray(it["points"][:, 0])).to(dev)
+                m = torch.empty(n * n, dtype=torch.float64, device=dev)
+                assert lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, 1, 2,
+                                                        it["length"], 0.0,
+                                                        C.c_void_p(m.data_ptr()), n,
+                                                        C.c_void_p(sh)) == 0
+                mats.append(m)
+            stream.synchronize()
+            t0 = time.perf_counter()
+            bt = DeviceTree.build_batched([m.data_ptr() for m in mats], [it["n"] for it in grp],
+                                          [it["n"] for it in grp], [it["height"] for it in grp],
+                                          1e-8, stream=sh)
+            stream.synchronize()
+            batched_s += time.perf_counter() - t0
+            for j, t in enumerate(bt):
+                rank_mismatch += int(np.any(t.ranks() != trees[g0 + j].ranks()))
+                t.free()
+            del mats
+            torch.cuda.empty_cache()
+    batched_s = multi.max_over_ranks(batched_s, pg, dev)
     storage = multi.sum_over_ranks(sum(t.info()["storage"] for t in trees), pg, dev)
     bytes_step = multi.sum_over_ranks(8.0 * sum(t.info()["storage"] for t in trees) +
                                       sum(16.0 * n * k for n, k in zip(ns, ks)), pg, dev)
@@ -489,7 +520,12 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, r
     out = {"instances": count, "ranks": world, "partition": "instance i on rank i mod ranks",
            "sizes": sorted(set(ns)), "k_range": [min(ks), max(ks)],
            "kernel": "exp(-|x-y|/l), l ~ U[0.05,0.5], sorted 1D points, seed 2",
-           "build_s_total": build_s, "storage_doubles": storage, "bytes_per_step": bytes_step,
+           "build_s_total": build_s,
+           "build_batched": {"seconds": batched_s, "group": group,
+                             "speedup_vs_per_tree": build_s / max(batched_s, 1e-9),
+                             "trees_with_other_ranks": rank_mismatch,
+                             "entry": "hodlr_b200_build_batched_dev"},
+           "storage_doubles": storage, "bytes_per_step": bytes_step,
            "loop_fp64": loop, "batched_fp64": b64, "batched_mixed": bmx,
            "speedup_batched_mixed_vs_loop_fp64": loop["ms_per_step"] / bmx["ms_per_step"],
            "rel_err_batched_fp64_vs_loop": (numb / den) ** 0.5,
