@@ -44,7 +44,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=None, help="override n (testing only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-n", type=int, default=4096)
+    ap.add_argument("--cpu-n", type=int, default=8192,
+                    help="n of the in-run CPU baseline sample (our arm)")
+    ap.add_argument("--ref-n", type=int, default=16384,
+                    help="n of the reference arm: the largest power of two the unmodified "
+                         "reference builds")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the n = 1024 H x and n = 16384 H x H measurements")
     ap.add_argument("--batch", type=int, default=512,
@@ -169,12 +173,12 @@ def int8_peak_tops(torch, dev):
         return 2.0 * bf16, "2 x measured BF16 dense peak (int8 GEMM unavailable)"
 
 
-def run_cpu_baseline(n: int, k: int, steps: int = 3, warmup: int = 1):
+def run_cpu_baseline(n: int, k: int, steps: int = 3, warmup: int = 1, extra=()):
     cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--n", str(n),
            "--height", str(max(1, (n // 128).bit_length() - 1)), "--k", str(k),
-           "--steps", str(steps), "--warmup", str(warmup)]
+           "--steps", str(steps), "--warmup", str(warmup), *extra]
     try:
-        out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+        out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1500)
         line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
         return json.loads(line)
     except Exception as e:  # the baseline is reported, never required
@@ -541,10 +545,13 @@ def reference_arm(args, rank):
     oracle/_ref) on this box's host cores, same metric and unit."""
     if rank != 0:
         return
-    # every step is one multiply_hodlr_dense of the bounded sample (n = 4096,
-    # about 25 ms on 8 cores), so K steps stay within seconds to minutes
+    # every step is one multiply_hodlr_dense of the reference's own build of
+    # the workload's kernel family at n = 16384 (the largest power of two its
+    # constructor reaches; its factors, about 170 MB, exceed the host caches
+    # like the n = 32768 tree's); building it takes the reference a few
+    # minutes, the K steps about a tenth of a second each
     steps, warmup = max(1, args.steps), max(0, args.warmup)
-    res = run_cpu_baseline(args.cpu_n, 256, steps, warmup)
+    res = run_cpu_baseline(args.ref_n, 256, steps, warmup, extra=("--batch-sample", "2"))
     if "error" in res:
         print(json.dumps({"impl": "reference", "unavailable": res["error"]}))
         return
@@ -565,6 +572,7 @@ def reference_arm(args, rank):
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": nthreads,
                          "kind": "reference", "sample": sample, "cpu": res.get("cpu")},
         "matvec_n1024_us": res.get("matvec_n1024_us"), "hxh_n4096_s": res.get("hxh_n4096_s"),
+        "batch_sample": res.get("batch_sample"),
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -70,6 +70,20 @@ def kernel_matrix(points: np.ndarray, kind: str, length: float, diag: float) -> 
     return np.asfortranarray(a)
 
 
+def kernel_matrix_blocked(points: np.ndarray, kind: str, length: float, diag: float,
+                          cols: int = 512) -> np.ndarray:
+    """kernel_matrix built a block of columns at a time (column-major), so
+    large n needs no n x n x dim temporaries."""
+    n = points.shape[0]
+    a = np.empty((n, n), order="F")
+    for j0 in range(0, n, cols):
+        j1 = min(n, j0 + cols)
+        d = points[:, None, :] - points[None, j0:j1, :]
+        a[:, j0:j1] = kernel_values(kind, np.sqrt(np.einsum("ijk,ijk->ij", d, d)), length)
+    a[np.arange(n), np.arange(n)] += diag
+    return a
+
+
 # ------------------------------------------------- benchmark workloads ---
 
 # The five workload shapes: (points, kernel, length, diagonal shift,
