@@ -187,13 +187,26 @@ def run_cpu_baseline(n: int, k: int, steps: int = 3, warmup: int = 1, extra=()):
 
 def build_stats(lib):
     """Stage times and counters of the calling thread's latest build."""
-    st = (C.c_double * 16)()
-    lib.hodlr_b200_build_stats(st, 16)
+    st = (C.c_double * 18)()
+    lib.hodlr_b200_build_stats(st, 18)
     return {"library_seconds": st[3], "exact_blocks": int(st[0]),
             "sketched_blocks": int(st[1]), "sketch_rounds": int(st[2]),
             "largest_sketch": int(st[9]), "ms_small_svd": st[10], "ms_rounds": st[11],
             "ms_core_svd": st[12], "ms_finish": st[13], "learned_fallbacks": int(st[14]),
-            "ms_features": st[15]}
+            "ms_features": st[15], "gemm_flops": st[16], "input_elems": st[17]}
+
+
+def build_roofline(stats, seconds, storage, peak_tflops, peak_gbs, matrix_free=False):
+    """Build against both roofs: its algorithmic bytes (the input read once,
+    8 n^2, unless matrix-free, plus the factors written once, 8 W) over the
+    wall time against the measured HBM bandwidth, and the FP64 GEMM work it
+    issued over the wall time against the FP64 GEMM peak measured in the run."""
+    nbytes = (0.0 if matrix_free else 8.0 * stats["input_elems"]) + 8.0 * storage
+    tflops = stats["gemm_flops"] / seconds / 1e12
+    return {"algorithmic_bytes": nbytes, "GB/s": nbytes / seconds / 1e9,
+            "frac_hbm": nbytes / seconds / 1e9 / peak_gbs, "gemm_flops": stats["gemm_flops"],
+            "TFLOP/s": tflops, "frac_fp64": tflops / peak_tflops,
+            "peaks": "HBM copy bandwidth of the driver's measurement; cuBLAS DGEMM of this run"}
 
 
 def side_workloads(lib, torch, dev, stream, sh):
@@ -295,7 +308,7 @@ def side_workloads(lib, torch, dev, stream, sh):
     return out
 
 
-def exp3d_workload(lib, torch, dev, stream, steps, warmup):
+def exp3d_workload(lib, torch, dev, stream, steps, warmup, peak64=None):
     """The learned-rank workload: n = 65536 points of [0,1]^3 (seed 4) in
     Morton order, exp(-r / 0.15) + 1e-2 I, depth 9 (leaf 128), tol 1e-8,
     k = 128 right-hand sides.  Both trees are built from the points
@@ -394,7 +407,10 @@ def exp3d_workload(lib, torch, dev, stream, steps, warmup):
         "build": {"plain": dict(seconds=plain_s, **plain_st),
                   "learned": dict(seconds=learned_s, **learned_st,
                                   max_rank_diff_vs_plain=int(np.max(np.abs(ranks_l - ranks)))),
-                  "speedup_learned_vs_plain": plain_s / learned_s},
+                  "speedup_learned_vs_plain": plain_s / learned_s,
+                  "roofline_plain": (build_roofline(plain_st, plain_s, info["storage"], peak64,
+                                                    measured_peaks().get("hbm_gbs", 6650.0),
+                                                    matrix_free=True) if peak64 else None)},
         "ranks_by_depth": by_depth(ranks), "ranks_by_depth_learned": by_depth(ranks_l),
         "factor_bytes": 8 * info["storage"], "max_rank": info["max_rank"],
         "matmat": {"fp64": r64, "mixed": rmx, "bytes_per_step": bytes_step,
@@ -828,7 +844,8 @@ def main():
 
     exp3d = None
     if not args.no_exp3d:
-        exp3d = exp3d_workload(lib, torch, dev, stream, args.steps, args.warmup)
+        exp3d = exp3d_workload(lib, torch, dev, stream, args.steps, args.warmup,
+                               fp64_peak_tflops(torch, dev))
 
     batch = None
     if args.batch > 0:
@@ -926,7 +943,12 @@ def main():
                                       **mf_stats),
                   "speedup_learned_vs_plain": build_s / build_s_learned,
                   "model": "hmat_lib_b200/rank_model.f32 (MLP 8-64-64-1, trained by the "
-                           "library's GPU kernels)"},
+                           "library's GPU kernels)",
+                  "roofline_plain": build_roofline(plain_stats, build_s, storage, peak64,
+                                                   measured_peaks().get("hbm_gbs", 6650.0)),
+                  "roofline_learned": build_roofline(learned_stats, build_s_learned, storage,
+                                                     peak64,
+                                                     measured_peaks().get("hbm_gbs", 6650.0))},
         "rel_err_vs_dense": rel_err,
         "rel_err_mixed_vs_fp64": rel_err_mixed_vs_fp64,
         "solve": solve_info,

@@ -854,7 +854,8 @@ int hodlr_b200_build_stats(double *out, int capacity) {
                       (double)st.failed_sketch,    (double)st.max_sketch,
                       st.ms_exact,                 st.ms_rounds,
                       st.ms_core_svd,              st.ms_finish,
-                      (double)st.learned_fallbacks, st.ms_features};
+                      (double)st.learned_fallbacks, st.ms_features,
+                      st.gemm_flops,               st.input_elems};
   const int n = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < n && i < capacity && out; ++i) out[i] = v[i];
   return n;

@@ -188,6 +188,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
                                                      int *svd_status, BuildStats *stats,
                                                      const KernelSpec *gen) {
   auto t0 = std::chrono::steady_clock::now();
+  gemm_flops_counter() = 0.0;
   HB_REQUIRE(!in.empty(), INPUT_ERROR, "build: no tree to build");
   HB_REQUIRE(!gen || in.size() == 1, INPUT_ERROR, "a matrix-free build takes one tree");
   *svd_status = SUCCESS;
@@ -864,6 +865,8 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
     }
   }
   st.ms_features = ms_features;
+  st.gemm_flops = gemm_flops_counter();
+  for (const Geometry &g : gs) st.input_elems += (double)g.n * g.n;
   st.ms_exact = stage_ms[0];
   st.ms_rounds = stage_ms[1];
   st.ms_core_svd = stage_ms[2];

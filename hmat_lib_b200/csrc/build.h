@@ -24,6 +24,8 @@ struct BuildStats {
   double ms_finish = 0.0;      // arena, leaf copies, U = Q U_R S, V = P V_R
   int learned_fallbacks = 0;   // one-shot sketches that failed the error check
   double ms_features = 0.0;    // rank-model features and prediction (host clock)
+  double gemm_flops = 0.0;     // FP64 GEMM work of the build (2 M N K summed)
+  double input_elems = 0.0;    // entries of the input matrices (n^2 per tree)
 };
 
 // Statistics of the most recent build on the calling thread.

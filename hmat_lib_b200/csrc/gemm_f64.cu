@@ -17,6 +17,11 @@ namespace hb {
 
 int gemm_f64_engine() { return (int)option("gemm_f64_engine", 1); }
 
+double &gemm_flops_counter() {
+  static thread_local double flops = 0.0;
+  return flops;
+}
+
 namespace {
 
 constexpr int kBK = 16;
@@ -529,6 +534,7 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
   double work = 0.0;
   for (size_t p = 0; p < probs.size(); ++p) {
     for (int s = 0; s < probs[p].nseg; ++s) ktot[p] += batch.segs[probs[p].seg0 + s].K;
+    gemm_flops_counter() += 2.0 * probs[p].M * (double)probs[p].N * (double)ktot[p];
     const long long mn =
         (long long)((probs[p].M + BM - 1) / BM) * ((probs[p].N + BN - 1) / BN);
     base_tiles += mn;

@@ -118,6 +118,10 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
 // Launches a plan: the beta pre-pass for split problems, then the GEMM.
 void gemm_plan_run(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stream);
 
+// FP64 multiply-add work (2 M N K per problem) of every GEMM plan built on
+// the calling thread since the counter was last reset (build statistics).
+double &gemm_flops_counter();
+
 // Which kernel runs the FP64 products (option gemm_f64_engine): 1 the FP64
 // tensor-core (DMMA) kernel, 0 the DFMA kernel.
 int gemm_f64_engine();

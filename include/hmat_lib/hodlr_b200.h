@@ -197,7 +197,8 @@ int hodlr_b200_phase_times(double *out, int capacity);
  * then the device milliseconds of the stages: small-block SVDs, sketch
  * rounds, SVDs of the sketched cores, finishing; one-shot sketches that fell
  * back to adaptive growth; milliseconds of the rank-model features and
- * prediction.  Returns the number of values. */
+ * prediction; FP64 GEMM work (flops, 2 M N K summed) and input entries.
+ * Returns the number of values. */
 int hodlr_b200_build_stats(double *out, int capacity);
 /* y = H x on device buffers, allocating nothing (no counterpart in hmat_lib).
  * For callers that cannot allocate device memory while they run: an
