@@ -281,6 +281,11 @@ std::shared_ptr<DeviceTree> hxh_multiply(DeviceTree &A, DeviceTree &B, double to
              "multiply_hodlr_hodlr: trees of different heights or block sizes");
   const int h = ga.h, nb = ga.nblock(), nleaf = ga.nleaf(), n = ga.n;
   const int dense_max = (int)option("hxh_dense_max", 256);
+  // option hxh_precision = 1: the subtree products (the bulk of the product's
+  // multiply-adds) on the int8 tensor cores; cores, recompression and leaves
+  // stay FP64.  Needs leaves that are multiples of 32.
+  bool mixed = option("hxh_precision", 0.0) == 1.0;
+  for (int m : ga.leaf_m) mixed = mixed && (m % 32 == 0);
 
   // ---- workspace layout --------------------------------------------------------
   long long ws = 0;
@@ -403,10 +408,18 @@ std::shared_ptr<DeviceTree> hxh_multiply(DeviceTree &A, DeviceTree &B, double to
           cp.push_back(CopyDesc{A.arena + ao.v_off, ao.n, work + xpd[d] + ao.c0, n, ao.n, ao.s});
       }
     run_copies(cp, s);
-    if (smax_b[d] > 0)
-      product_f64(A, ProdOp::N, work + xd[d], smax_b[d], n, work + yd[d], n, s, d + 1);
-    if (smax_a[d] > 0)
-      product_f64(B, ProdOp::T, work + xpd[d], smax_a[d], n, work + ypd[d], n, s, d + 1);
+    if (smax_b[d] > 0) {
+      if (mixed)
+        product_mixed_op(A, ProdOp::N, work + xd[d], smax_b[d], n, work + yd[d], n, s, d + 1);
+      else
+        product_f64(A, ProdOp::N, work + xd[d], smax_b[d], n, work + yd[d], n, s, d + 1);
+    }
+    if (smax_a[d] > 0) {
+      if (mixed)
+        product_mixed_op(B, ProdOp::T, work + xpd[d], smax_a[d], n, work + ypd[d], n, s, d + 1);
+      else
+        product_f64(B, ProdOp::T, work + xpd[d], smax_a[d], n, work + ypd[d], n, s, d + 1);
+    }
   }
 
   // ---- 3. concatenated factors ---------------------------------------------------------

@@ -51,14 +51,16 @@ void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx
                  long long ldy, cudaStream_t stream, int min_depth = 0);
 
 // Mixed-precision Y = H X (op N) on the int8 tensor cores (products_mixed.cu).
+// With min_depth > 0 only the leaves and the blocks of depth >= min_depth
+// take part (as for product_f64).
 void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double *Y,
-                   long long ldy, cudaStream_t stream);
+                   long long ldy, cudaStream_t stream, int min_depth = 0);
 // Mixed-precision Y = op(H, X) for every op: H^T X is the op-N product of the
 // cached transposed tree (leaves D^T, each block the transpose of its
 // sibling), X H = (H^T X^T)^T with X and the result transposed through
 // device scratch.
 void product_mixed_op(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx,
-                      double *Y, long long ldy, cudaStream_t stream);
+                      double *Y, long long ldy, cudaStream_t stream, int min_depth = 0);
 // Error word of the tree's mixed-precision kernels (0: none), read and reset.
 int mixed_status(DeviceTree &t, cudaStream_t stream);
 

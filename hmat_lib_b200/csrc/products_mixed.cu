@@ -94,7 +94,7 @@ struct MixedState {
   std::vector<long long> vb_off;           // per block: bytes of its first B tile
   std::vector<int> nw, ntn;                // per block: B tile width, number of tiles
   std::vector<long long> gexp;             // per block: offset of its column exponents
-  std::map<std::tuple<int, long long, long long>, std::unique_ptr<MixedPlan>> plans;
+  std::map<std::tuple<int, long long, long long, int>, std::unique_ptr<MixedPlan>> plans;
   ~MixedState();
 };
 
@@ -224,13 +224,17 @@ MixedState &mixed_state(DeviceTree &t, cudaStream_t s) {
 }
 
 MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long long ldy,
-                      cudaStream_t s) {
-  auto key = std::make_tuple(k, ldx, ldy);
+                      cudaStream_t s, int min_depth = 0) {
+  auto key = std::make_tuple(k, ldx, ldy, min_depth);
   auto it = st.plans.find(key);
   if (it != st.plans.end()) return *it->second;
   const Geometry &g = t.g;
   const int n = g.n, nb = g.nblock(), nl = g.nleaf(), h = g.h;
   const int nkbn = n / kOzKBlock;
+  // blocks that take part: nonzero rank, depth >= min_depth (a product of
+  // the leaves and the deeper blocks only: the block-diagonal product of
+  // the subtrees rooted at min_depth)
+  auto inc = [&](int b) { return g.blocks[b].s > 0 && g.blocks[b].depth >= min_depth; };
   auto plan = std::make_unique<MixedPlan>();
   MixedPlan &P = *plan;
   P.k = k;
@@ -250,7 +254,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   // ---- phase 1 tiles: split long blocks along K so the work spreads -------------
   long long work = 0;
   for (int b = 0; b < nb; ++b)
-    if (g.blocks[b].s) work += (long long)st.ntn[b] * st.nw[b] * (g.blocks[b].n / kOzKBlock);
+    if (inc(b)) work += (long long)st.ntn[b] * st.nw[b] * (g.blocks[b].n / kOzKBlock);
   work *= nja;
   // about `per_cta` tiles' worth of work per CTA (option ozaki_phase1_tiles_per_cta)
   const long long per_cta = std::max(1LL, (long long)option("ozaki_phase1_tiles_per_cta", 2.0));
@@ -258,7 +262,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   std::vector<int> nch(nb, 1);
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
-    if (!B.s) continue;
+    if (!inc(b)) continue;
     const int nkb = B.n / kOzKBlock;
     nch[b] = (int)std::max(1LL, std::min<long long>(nkb / 8, cdiv((long long)st.nw[b] * nkb, target)));
     nch[b] = (int)std::max<long long>(nch[b], cdiv(nkb, kOzMaxK / kOzKBlock));
@@ -269,7 +273,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   for (int pass = 0; pass < 2; ++pass)
     for (int b = 0; b < nb; ++b) {
       const BlockDesc &B = g.blocks[b];
-      if (!B.s || (nch[b] > 1) != (pass == 0)) continue;
+      if (!inc(b) || (nch[b] > 1) != (pass == 0)) continue;
       w_off[b] = wd;
       wd += align_up((long long)B.s * k);
       if (pass == 0) P.w_zero = wd;
@@ -280,7 +284,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   std::vector<long long> work1;
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
-    if (!B.s) continue;
+    if (!inc(b)) continue;
     const int nkb = B.n / kOzKBlock, nw = st.nw[b];
     const int per = (int)cdiv(nkb, nch[b]);
     for (int tn = 0; tn < st.ntn[b]; ++tn)
@@ -319,7 +323,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   long long wbb = 0;
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
-    if (!B.s) continue;
+    if (!inc(b)) continue;
     wb_off[b] = wbb;
     wbb += (long long)njb * (pad32(B.s) / kOzKBlock) * oz_bblock(P.nw2);
   }
@@ -354,10 +358,12 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
           const BlockDesc &B = g.blocks[b];
           if (!B.s) continue;
           const int nks = pad32(B.s) / kOzKBlock;
-          s2.push_back(
-              OzSeg{a, P.wb + wb_off[b] + (long long)jb * nks * oz_bblock(P.nw2), nks, 0});
+          if (B.depth >= min_depth) {
+            s2.push_back(
+                OzSeg{a, P.wb + wb_off[b] + (long long)jb * nks * oz_bblock(P.nw2), nks, 0});
+            ++tl.nseg;
+          }
           a += (long long)nks * kOzABlock;
-          ++tl.nseg;
         }
         t2.push_back(tl);
       }
@@ -373,7 +379,7 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
   std::vector<SliceJob> sb;
   for (int b = 0; b < nb; ++b) {
     const BlockDesc &B = g.blocks[b];
-    if (!B.s) continue;
+    if (!inc(b)) continue;
     const double *wt = P.w + w_off[b];
     if (nch[b] > 1) mw.push_back(MaxJob{wt, 1, k, k, B.s, P.fmax, 0});
     const int nks = pad32(B.s) / kOzKBlock;
@@ -430,12 +436,12 @@ MixedPlan &mixed_plan(DeviceTree &t, MixedState &st, int k, long long ldx, long 
 }  // namespace
 
 void product_mixed(DeviceTree &t, const double *X, int k, long long ldx, double *Y, long long ldy,
-                   cudaStream_t s) {
+                   cudaStream_t s, int min_depth) {
   if (k <= 0 || t.g.n == 0) return;
   HB_REQUIRE(ldx >= t.g.n && ldy >= t.g.n, INPUT_ERROR, "leading dimension below n");
   std::lock_guard<std::mutex> lk(t.plan_mutex);
   MixedState &st = mixed_state(t, s);
-  MixedPlan &P = mixed_plan(t, st, k, ldx, ldy, s);
+  MixedPlan &P = mixed_plan(t, st, k, ldx, ldy, s, min_depth);
   PhaseTimer timer(s);
   // 1. exponents and slices of X for phase 1; W^T = X^T V per block (the
   //    epilogue also folds the column maxima of unsplit blocks into fmax)
@@ -533,9 +539,9 @@ DeviceTree &transposed_tree(DeviceTree &t, cudaStream_t s) {
 }  // namespace
 
 void product_mixed_op(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
-                      long long ldy, cudaStream_t s) {
+                      long long ldy, cudaStream_t s, int min_depth) {
   if (op == ProdOp::N) {
-    product_mixed(t, X, k, ldx, Y, ldy, s);
+    product_mixed(t, X, k, ldx, Y, ldy, s, min_depth);
     return;
   }
   if (k <= 0 || t.g.n == 0) return;
@@ -545,7 +551,7 @@ void product_mixed_op(DeviceTree &t, ProdOp op, const double *X, int k, long lon
     tt = &transposed_tree(t, s);
   }
   if (op == ProdOp::T) {
-    product_mixed(*tt, X, k, ldx, Y, ldy, s);
+    product_mixed(*tt, X, k, ldx, Y, ldy, s, min_depth);
     return;
   }
   // X H with X k x n (ld ldx): (X H)^T = H^T X^T
@@ -555,7 +561,7 @@ void product_mixed_op(DeviceTree &t, ProdOp op, const double *X, int k, long lon
   double *yt = xt + (size_t)n * k;
   transpose(X, ldx, k, n, xt, n, s);
   try {
-    product_mixed(*tt, xt, k, n, yt, n, s);
+    product_mixed(*tt, xt, k, n, yt, n, s, min_depth);
   } catch (...) {
     dev_free(xt, s);
     throw;

@@ -83,6 +83,8 @@ const char *hodlr_b200_last_error(void);
  *       the block Jacobi SVD (16-column blocks, QR + small SVD + GEMM rounds)
  *   hxh_dense_max (256): H x H blocks up to this many rows are recompressed
  *       from their dense product
+ *   hxh_precision (0): 1 = the subtree products of H x H on the int8 tensor
+ *       cores (cores, recompression and leaves stay FP64)
  *   autotune (1), batch_shape (-1), use_graphs (1), check_status (0): batched
  *       products time candidate tile shapes / force one (0-3) / replay a CUDA
  *       graph / read the mixed kernels' status word after each call

@@ -134,3 +134,31 @@ def test_device_recompress_known_answers(c):
             sgn = 1.0 if np.dot(ru[:, j], eu[:, j]) >= 0 else -1.0
             assert np.abs(sgn * ru[:, j] - eu[:, j]).max() <= 1e-9
             assert np.abs(sgn * rv[:, j] - ev[:, j]).max() <= 1e-9
+
+
+def test_hxh_with_int8_subtree_products(lib):
+    """Option hxh_precision = 1 runs the subtree products of H x H (depth-
+    masked products: leaves and the blocks below each depth) on the int8
+    tensor cores: same ranks as the FP64 product within one, and the
+    product's action within 1e-10 of the FP64 product's and within 2 tol of
+    the dense A (B X)."""
+    n, h, tol = 2048, 4, 1e-8
+    pts = W.points_1d_sorted(n, seed=3)
+    a = W.kernel_matrix(pts, "gaussian", 0.1, 1.0)
+    b = W.kernel_matrix(pts, "matern32", 0.2, 1.0)
+    ta, tb = Tree.from_dense(a, h, tol), Tree.from_dense(b, h, tol)
+    tc64 = ta.hxh(tb, tol)
+    lib.hodlr_b200_set_option(b"hxh_precision", 1.0)
+    try:
+        tcmx = ta.hxh(tb, tol)
+    finally:
+        lib.hodlr_b200_set_option(b"hxh_precision", 0.0)
+    r64 = np.array([u.shape[1] for _, (u, _) in sorted(tc64.data().blocks.items())])
+    rmx = np.array([u.shape[1] for _, (u, _) in sorted(tcmx.data().blocks.items())])
+    assert int(np.abs(r64 - rmx).max()) <= 1
+    x = np.asfortranarray(np.random.default_rng(1).standard_normal((n, 6)))
+    y64, ymx = tc64.matmat(x), tcmx.matmat(x)
+    assert O.rel_fro(ymx, y64) < 1e-10
+    assert O.rel_fro(ymx, a @ (b @ x)) < 2 * tol
+    for t in (tcmx, tc64, tb, ta):
+        t.free()
