@@ -294,12 +294,38 @@ def side_workloads(lib, torch, dev, stream, sh):
         yd = (xk @ db) @ da                        # rows of (A (B X))^T; A, B symmetric
         stream.synchronize()
         cinfo = tc.info()
+        # the same product with its subtree products on the int8 tensor cores
+        lib.hodlr_b200_set_option(b"hxh_precision", 1.0)
+        try:
+            tm = ta.hxh(tb, tol)                  # warm-up: slices and plans
+            tm.free()
+            torch.cuda.synchronize()
+            times_mx = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                tm = ta.hxh(tb, tol)
+                torch.cuda.synchronize()
+                times_mx.append(time.perf_counter() - t0)
+                if len(times_mx) < 3:
+                    tm.free()
+        finally:
+            lib.hodlr_b200_set_option(b"hxh_precision", 0.0)
+        ym = torch.zeros_like(xk)
+        tm.matmat(xk.data_ptr(), 16, n, ym.data_ptr(), n, stream=sh)
+        stream.synchronize()
         out["hxh_n16384"] = {
             "seconds": min(times), "height": h, "tol": tol,
             "max_rank_out": cinfo["max_rank"],
             "rel_err_vs_dense": (torch.linalg.norm(yc - yd) / torch.linalg.norm(yd)).item(),
             "rel_err_vs_factors_product": (torch.linalg.norm(yc - yh) / torch.linalg.norm(yh)).item(),
+            "mixed_subtree_products": {
+                "seconds": min(times_mx),
+                "rel_err_vs_dense": (torch.linalg.norm(ym - yd) / torch.linalg.norm(yd)).item(),
+                "rel_err_vs_fp64_product": (torch.linalg.norm(ym - yc) /
+                                            torch.linalg.norm(yc)).item(),
+                "option": "hxh_precision=1"},
             "check": "(H_A H_B) X vs A (B X) with the dense kernel matrices, X n x 16"}
+        tm.free()
         tc.free()
         ta.free()
         tb.free()
