@@ -14,6 +14,7 @@ std::unordered_map<const TreeHODLR *, std::shared_ptr<DeviceTree>> g_registry;
 }  // namespace
 
 DeviceTree::~DeviceTree() {
+  graphs.clear();
   plans.clear();
   mixed.reset();
   transposed.reset();

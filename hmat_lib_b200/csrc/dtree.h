@@ -17,6 +17,16 @@ namespace hb {
 struct ProductPlan;
 struct MixedState;
 
+// A captured launch sequence of one product (CUDA graph), replayed by later
+// calls with the same tree, op, sizes, buffers and stream.
+struct ProductGraph {
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;     // kernels in the graph (for the launch counter)
+  ~ProductGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
 struct DeviceTree {
   int device = 0;
   Geometry g;                       // blocks carry u_off / v_off into `arena`
@@ -27,6 +37,11 @@ struct DeviceTree {
   BlockDesc *d_blocks = nullptr;
   uint64_t fingerprint = 0;         // of the host tree this mirrors (0: none)
   std::map<std::tuple<int, int, long long, long long, int, int>, std::unique_ptr<ProductPlan>> plans;
+  // (op, k, ldx, ldy, min_depth, X, Y, stream) -> graph; an entry holding
+  // nullptr marks a signature seen once (captured on its second call)
+  std::map<std::tuple<int, int, long long, long long, int, const void *, void *, void *>,
+           std::unique_ptr<ProductGraph>>
+      graphs;
   std::mutex plan_mutex;
   std::shared_ptr<MixedState> mixed;   // int8 slices of the factors (mixed precision)
   std::shared_ptr<DeviceTree> transposed;   // H^T with the same geometry (mixed op T / L)

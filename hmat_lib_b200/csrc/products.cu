@@ -210,8 +210,82 @@ int phase_times(double *out, int cap) {
   return 5;
 }
 
+namespace {
+
+// Runs `launch` (the kernel launches of one product) directly, or as a CUDA
+// graph: the first call of a signature runs directly (lazy plans and scratch
+// are made then), the second is captured on `stream` and replayed, later ones
+// only replay.  Not with the legacy default stream, inside a caller's stream
+// capture, with phase timing on, or with option product_graphs = 0.
+template <class F>
+void run_graphed(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy, int min_depth,
+                 const double *X, double *Y, cudaStream_t stream, F launch) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool graphable = stream != nullptr && option("product_graphs", 1.0) != 0.0 &&
+                         option("record_phase_times", 0.0) == 0.0 &&
+                         cudaStreamIsCapturing(stream, &cs) == cudaSuccess &&
+                         cs == cudaStreamCaptureStatusNone;
+  if (!graphable) {
+    (void)cudaGetLastError();
+    launch();
+    return;
+  }
+  const auto key = std::make_tuple((int)op, k, ldx, ldy, min_depth, (const void *)X, (void *)Y,
+                                   (void *)stream);
+  std::unique_ptr<ProductGraph> *slot;
+  {
+    std::lock_guard<std::mutex> lk(t.plan_mutex);
+    auto it = t.graphs.find(key);
+    if (it == t.graphs.end()) {
+      if (t.graphs.size() >= 256) t.graphs.clear();   // bounded cache
+      t.graphs.emplace(key, nullptr);                 // seen once
+      slot = nullptr;
+    } else {
+      slot = &it->second;
+    }
+  }
+  if (!slot) {
+    launch();
+    return;
+  }
+  if (!*slot) {
+    const long long l0 = launches();
+    cudaGraph_t graph = nullptr;
+    HB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      launch();
+    } catch (...) {
+      cudaStreamEndCapture(stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      throw;
+    }
+    HB_CUDA(cudaStreamEndCapture(stream, &graph));
+    auto pg = std::make_unique<ProductGraph>();
+    pg->launches = launches() - l0;
+    const cudaError_t e = cudaGraphInstantiate(&pg->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    HB_CUDA(e);
+    *slot = std::move(pg);
+    // the captured launches were counted when captured; the replay below
+    // counts them again as run
+    count_launch(-(*slot)->launches);
+  }
+  HB_CUDA(cudaGraphLaunch((*slot)->exec, stream));
+  count_launch((*slot)->launches);
+}
+
+}  // namespace
+
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
                  long long ldy, cudaStream_t stream, int min_depth) {
+  if (k <= 0 || t.g.n == 0) return;
+  run_graphed(t, op, k, ldx, ldy, min_depth, X, Y, stream,
+              [&] { product_f64_direct(t, op, X, k, ldx, Y, ldy, stream, min_depth); });
+}
+
+void product_f64_direct(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
+                        long long ldy, cudaStream_t stream, int min_depth) {
   if (k <= 0 || t.g.n == 0) return;
   // one vector: the HBM-bound matvec kernels (option matvec_kernels = 0 keeps
   // the GEMM engine)

@@ -49,6 +49,10 @@ ProductWork product_work(const DeviceTree &t, int k);
 // rooted at that depth (used by HODLR x HODLR).
 void product_f64(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx, double *Y,
                  long long ldy, cudaStream_t stream, int min_depth = 0);
+// The same, always launched directly (product_f64 replays a captured graph
+// when a call repeats an earlier one's tree, op, sizes, buffers and stream).
+void product_f64_direct(DeviceTree &t, ProdOp op, const double *X, int k, long long ldx,
+                        double *Y, long long ldy, cudaStream_t stream, int min_depth = 0);
 
 // Mixed-precision Y = H X (op N) on the int8 tensor cores (products_mixed.cu).
 // With min_depth > 0 only the leaves and the blocks of depth >= min_depth

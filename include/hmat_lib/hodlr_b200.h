@@ -94,7 +94,10 @@ const char *hodlr_b200_last_error(void);
  *   record_phase_times (0): events around each product phase and its main GEMM
  *       (hodlr_b200_phase_times)
  *   gemm_f64_engine (1): FP64 products on the FP64 tensor cores (DMMA); 0 =
- *       the DFMA kernel */
+ *       the DFMA kernel
+ *   product_graphs (1): a device FP64 product that repeats an earlier call
+ *       (same tree, op, sizes, buffers and non-default stream) is captured
+ *       once as a CUDA graph and replayed; 0 = always launch directly */
 int hodlr_b200_set_option(const char *name, double value);
 /* Allocator for every host buffer the library allocates (tree nodes, factor
  * copies, results returned for out == NULL).  Both NULL restores malloc/free. */

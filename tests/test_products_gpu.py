@@ -10,7 +10,7 @@ import pytest
 
 from hmat_lib_b200 import abi
 from hmat_lib_b200 import workloads as W
-from hmat_lib_b200.hodlr import Tree
+from hmat_lib_b200.hodlr import DeviceTree, Tree
 from hmat_lib_b200.tree import TreeData
 from oracle import hodlr_oracle as O
 
@@ -250,3 +250,45 @@ def test_single_vector_products(lib, use_kernels):
             t.free()
     finally:
         lib.hodlr_b200_set_option(b"matvec_kernels", 1.0)
+
+
+@pytest.mark.parametrize("k", [1, 24])
+def test_repeated_products_replay_graphs(lib, k):
+    """On a non-default stream, a product that repeats an earlier call (same
+    tree, op, sizes, buffers) is captured once as a CUDA graph and replayed:
+    new input values give the same results as direct launches (option
+    product_graphs = 0), and the library's launch counter still counts the
+    replayed kernels."""
+    import torch
+    n, h = 2048, 4
+    pts = W.points_morton(n, 2, seed=6)
+    a = W.kernel_matrix(pts, "matern32", 0.1, 1e-2)
+    t = Tree.from_dense(a, h, 1e-8)
+    dt = DeviceTree.of_host(t)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    x = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    rng = np.random.default_rng(k)
+    results = []
+    for it in range(5):
+        xv = rng.standard_normal((n, k))
+        x.copy_(torch.from_numpy(np.ascontiguousarray(xv.T)))
+        torch.cuda.synchronize()
+        l0 = lib.hodlr_b200_kernel_launches()
+        dt.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
+        stream.synchronize()
+        assert lib.hodlr_b200_kernel_launches() > l0
+        results.append((xv, y.cpu().numpy().T.copy()))
+    lib.hodlr_b200_set_option(b"product_graphs", 0.0)
+    try:
+        for xv, got in results:
+            x.copy_(torch.from_numpy(np.ascontiguousarray(xv.T)))
+            torch.cuda.synchronize()
+            dt.matmat(x.data_ptr(), k, n, y.data_ptr(), n, stream=sh)
+            stream.synchronize()
+            assert O.rel_fro(y.cpu().numpy().T, got) < 1e-14   # split-K atomics: rounding order
+    finally:
+        lib.hodlr_b200_set_option(b"product_graphs", 1.0)
+    dt.free()
+    t.free()
