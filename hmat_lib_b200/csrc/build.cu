@@ -26,6 +26,7 @@
 #include "build.h"
 #include "jacobi.h"
 #include "rank_mlp.h"
+#include "sketch_mixed.h"
 #include "tsqr.h"
 #include "workload.h"
 
@@ -60,6 +61,7 @@ struct SketchBlock {
   int pred = -1;         // predicted rank (-1: none)
   bool one_shot = false; // first round sized by the predictor, judged at tol
   bool fell_back = false;
+  int mix = -1;          // index in the int8 sketch products (-1: FP64 GEMMs)
 };
 
 thread_local BuildStats g_last_stats;
@@ -256,6 +258,23 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
     eslots.push_back(s);
     max_c = std::max(max_c, C);
   }
+  // Option build_precision = 1 (dense input only): the sketch products
+  // Y = A Omega and B^T = A^T Q on the int8 tensor cores, every block sliced
+  // once here (before the sketch widths are sized, so the slices count
+  // against the memory); blocks whose sizes are not multiples of 32 keep the
+  // FP64 GEMMs.
+  std::unique_ptr<SketchMixed> smix;
+  std::vector<int> mix_of(sketched.size(), -1);
+  if (!gen && option("build_precision", 0.0) == 1.0) {
+    std::vector<SketchMixedBlock> mb;
+    for (size_t si = 0; si < sketched.size(); ++si) {
+      const Blk &X = blk[sketched[si]];
+      if (X.B.m % 32 || X.B.n % 32) continue;
+      mix_of[si] = (int)mb.size();
+      mb.push_back(SketchMixedBlock{d_A + X.a0, X.lda, X.B.m, X.B.n});
+    }
+    if (!mb.empty()) smix = std::make_unique<SketchMixed>(mb, stream);
+  }
   // Sketch width caps.  Option sketch_cap > 0 fixes one cap for every block;
   // 0 (default) bounds them by memory: every sketched block may grow to
   // alpha min(m, n) columns (whole panels, at least two rounds' width), with
@@ -325,6 +344,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
     S.n = B.n;
     S.cap = caps[si];
     S.a_off = blk[b].a0;
+    S.mix = mix_of[si];
     sk.push_back(S);
   }
   // ---- learned sizing of the first sketch ---------------------------------------------
@@ -479,12 +499,19 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
     // 2. Y = A Om written into the new columns of Q; 3. Y -= Q (B Om)
     {
       GemmBatch g1;
+      std::vector<SketchMixed::Call> m1;
       for (int i : act) {
         const SketchBlock &S = sk[i];
+        if (S.mix >= 0) {
+          m1.push_back(SketchMixed::Call{S.mix, work + S.om, S.n, wb[i],
+                                         work + S.q + (long long)S.ell * S.m, S.m});
+          continue;
+        }
         int pr = g1.add(kWork, S.q + (long long)S.ell * S.m, S.m, S.m, wb[i]);
         g1.seg(pr, aslot, S.a_off, S.lda, 0, kWork, S.om, S.n, 0, S.n);
       }
       gemm_f64_run(g1, bases, TileShape::M128N64, stream);
+      if (smix) smix->multiply(false, m1, stream);
       // ||A om_c||^2: the scale against which a projected column counts as noise
       std::vector<NormDesc> nd;
       for (int i : act) {
@@ -596,12 +623,19 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
     // 5. B^T new columns = A^T Q_new; copy them to P for orthonormalisation
     {
       GemmBatch g5;
+      std::vector<SketchMixed::Call> m5;
       for (int i : act) {
         const SketchBlock &S = sk[i];
+        if (S.mix >= 0) {
+          m5.push_back(SketchMixed::Call{S.mix, work + S.q + (long long)S.ell * S.m, S.m, wb[i],
+                                         work + S.bt + (long long)S.ell * S.n, S.n});
+          continue;
+        }
         int pr = g5.add(kWork, S.bt + (long long)S.ell * S.n, S.n, S.n, wb[i]);
         g5.seg(pr, aslot, S.a_off, S.lda, 1, kWork, S.q + (long long)S.ell * S.m, S.m, 0, S.m);
       }
       gemm_f64_run(g5, bases, TileShape::M128N64, stream);
+      if (smix) smix->multiply(true, m5, stream);
       std::vector<CopyDesc> cp;
       for (int i : act) {
         const SketchBlock &S = sk[i];
@@ -827,6 +861,11 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
   dev_free(jwork, stream);
   dev_free(work, stream);
   HB_CUDA(cudaStreamSynchronize(stream));
+  if (smix && smix->status(stream) != SUCCESS) {
+    *svd_status = SVD_FAILURE;
+    set_last_error("an int8 sketch product gave up waiting on a barrier");
+  }
+  smix.reset();
   if (cap_hit) {
     *svd_status = SVD_FAILURE;
     set_last_error(cap_opt > 0

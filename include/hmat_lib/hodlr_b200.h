@@ -85,6 +85,9 @@ const char *hodlr_b200_last_error(void);
  *       from their dense product
  *   hxh_precision (0): 1 = the subtree products of H x H on the int8 tensor
  *       cores (cores, recompression and leaves stay FP64)
+ *   build_precision (0): 1 = the sketch products of a dense-input build
+ *       (Y = A Omega, B^T = A^T Q) on the int8 tensor cores; orthonormalisation,
+ *       core SVDs and truncation stay FP64
  *   autotune (1), batch_shape (-1), use_graphs (1), check_status (0): batched
  *       products time candidate tile shapes / force one (0-3) / replay a CUDA
  *       graph / read the mixed kernels' status word after each call
