@@ -870,8 +870,14 @@ def main():
 
     exp3d = None
     if not args.no_exp3d:
-        exp3d = exp3d_workload(lib, torch, dev, stream, args.steps, args.warmup,
-                               fp64_peak_tflops(torch, dev))
+        # reported, never required: a failure here is recorded in the line
+        try:
+            exp3d = exp3d_workload(lib, torch, dev, stream, args.steps, args.warmup,
+                                   fp64_peak_tflops(torch, dev))
+        except Exception as e:
+            exp3d = {"error": str(e)[:300]}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
 
     batch = None
     if args.batch > 0:

@@ -88,6 +88,7 @@ struct Work {
   int round = 0, sweep = 0;
   bool active = true, converged = false;
   double theta = 0.0;     // column norms at or below this are not rotated
+  double fro = 0.0;       // ||A||_F
 };
 
 }  // namespace
@@ -166,6 +167,7 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
       for (double v : h) f2 += v;
       // the scalar solver's skip rule for the relative truncation
       wk[p].theta = 1e-3 * tol * std::sqrt(f2) / wk[p].L;
+      wk[p].fro = std::sqrt(f2);
     }
   }
   GemmBases bases{};
@@ -224,6 +226,12 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
         j.rank = d_rank + W.slot0 + k;
         j.sweeps = d_sw + W.slot0 + k;
         j.skip_abs = W.theta;
+        // A pair's columns are recomputed by a GEMM every round, so a large
+        // and a small column keep a coupling of about eps ||A|| ||large||;
+        // such pairs count as orthogonal (singular values then carry an
+        // absolute error of that order, far below the truncation threshold
+        // tol ||A||), otherwise sweeps would never end.
+        j.conv_scale = W.fro;
         jp.push_back(j);
         // X[:, a] = Q (U_R S)[:, 0:16], X[:, b] = Q (U_R S)[:, 16:32]
         int q = gx.add(0, xa, L, (int)L, kBj);
@@ -323,6 +331,8 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
   if (failed) {
     const int st = SVD_FAILURE;
     HB_CUDA(cudaMemcpyAsync(d_status, &st, sizeof(int), cudaMemcpyHostToDevice, s));
+    set_last_error("block Jacobi SVD of a sketch core did not converge within "
+                   "jacobi_max_sweeps sweeps");
   }
   HB_CUDA(cudaStreamSynchronize(s));
   cudaFreeAsync(d_ints, s);

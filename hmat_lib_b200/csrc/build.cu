@@ -276,20 +276,24 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
     if (!mb.empty()) smix = std::make_unique<SketchMixed>(mb, stream);
   }
   // Sketch width caps.  Option sketch_cap > 0 fixes one cap for every block;
-  // 0 (default) bounds them by memory: every sketched block may grow to
-  // alpha min(m, n) columns (whole panels, at least two rounds' width), with
-  // alpha in (0, 1] the largest value whose scratch -- Q, B^T, P, R_B and the
-  // round buffers, plus the SVD of the core -- fits option sketch_mem_frac
-  // (default 0.6) of the device memory that is free or held unused by the
-  // stream-ordered pool.
+  // 0 (default) bounds them by memory: blocks of up to 2048 columns may grow
+  // to their full width, wider ones to alpha min(m, n) columns (whole panels,
+  // at least 2048), with alpha in (0, 1] the largest value whose scratch --
+  // Q, B^T, P, R_B and the round buffers, plus the SVD of the core -- fits
+  // option sketch_mem_frac (default 0.6) of the device memory that is free
+  // or held unused by the stream-ordered pool.
   std::vector<int> caps(sketched.size(), 0);
   {
     const int w_round = std::max(w_first, w_next);
+    // blocks up to kFullCap columns always get their whole width (their
+    // scratch is small); alpha applies to the wider ones
+    constexpr int kFullCap = 2048;
     auto cap_of = [&](const BlockDesc &B, double alpha) {
       const int C = std::min(B.m, B.n);
       if (cap_opt > 0) return std::min(C, std::max(cap_opt, kPanel));
+      if (C <= kFullCap) return C;
       const int c = (int)std::ceil(alpha * C / kPanel) * kPanel;
-      return std::min(C, std::max(c, 2 * w_round));
+      return std::min(C, std::max(c, kFullCap));
     };
     auto bytes_of = [&](double alpha) {
       double total = 0.0;

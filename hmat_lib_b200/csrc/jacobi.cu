@@ -196,7 +196,12 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
         ga = warp_sum(ga);
         if (ga == 0.0 || al <= 0.0 || be <= 0.0) continue;
         if (al <= skip2 || be <= skip2) continue;
-        const double rel = fabs(ga) / (sqrt(al) * sqrt(be));
+        double rel = fabs(ga) / (sqrt(al) * sqrt(be));
+        // coupling at rounding level of the problem's own scale (a block of a
+        // larger matrix, whose columns were recomputed by a GEMM) counts as
+        // converged: it moves no singular value by more than that level
+        if (P.conv_scale > 0.0)
+          rel = fmin(rel, fabs(ga) / (P.conv_scale * fmax(sqrt(al), sqrt(be))));
         off = fmax(off, rel);
         if (rel <= conv) continue;
         const double zeta = (be - al) / (2.0 * ga);

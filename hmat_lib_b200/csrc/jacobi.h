@@ -28,6 +28,8 @@ struct JacobiProb {
   int gen_c0 = 0;   //   (gen_r0, gen_c0) (element (i, j) computed, A / lda unused)
   double skip_abs = 0.0;   // pairs with a column norm at or below this are neither
                            // rotated nor tested (on top of the truncation's own rule)
+  double conv_scale = 0.0; // > 0: a pair also counts as orthogonal when
+                           // |g_p . g_q| <= conv_tol conv_scale max(||g_p||, ||g_q||)
 };
 
 enum class Truncation : int {

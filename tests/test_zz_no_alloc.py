@@ -6,7 +6,7 @@ fixed array of device memory inside the library.
 
 Checked through the C-ABI against the existing device product
 (hodlr_b200_matmat_dev with one right-hand side) on two calls in a row, on
-a single-leaf tree and on a tree whose blocks all have rank zero, and for the
+a height-1 tree and on a tree whose blocks all have rank zero, and for the
 clear rejection of trees beyond the array's capacity (too many ranks, too
 many blocks) before anything is launched.  Self-contained
 so it passes alone in a fresh process and after the other tests."""
@@ -108,17 +108,20 @@ def _random_tree(sizes, h, rank_of, seed=0):
     return td
 
 
-@pytest.mark.parametrize("case", ["single_leaf", "zero_ranks"])
+@pytest.mark.parametrize("case", ["one_level", "zero_ranks"])
 def test_noalloc_matvec_edge_trees(case):
-    """A tree of height 0 (one dense leaf, no off-diagonal block) and a tree
-    whose blocks all have rank 0 (no projection is launched): same result as
-    the existing device product and as the CPU oracle."""
+    """The smallest tree (height 1: two leaves, one rank-0 and one rank-5
+    block; hmat_lib's allocate_tree takes no height-0 tree) and a tree whose
+    blocks all have rank 0 (no projection is launched): same result as the
+    existing device product and as the CPU oracle."""
     import torch
 
     lib = abi.load()
-    if case == "single_leaf":
-        n, h = 200, 0
-        td = _random_tree([n], h, lambda d, top: 0, seed=1)
+    if case == "one_level":
+        n, h = 200, 1
+        td = _random_tree([100, 100], h, lambda d, top: 0, seed=1)
+        rng = np.random.default_rng(11)
+        td.blocks[(0, 0, 2)] = (rng.standard_normal((100, 5)), rng.standard_normal((100, 5)))
     else:
         n, h = 1000, 3
         td = _random_tree(O.block_sizes_halves(n, h), h, lambda d, top: 0, seed=2)
