@@ -23,6 +23,7 @@
 #include "jacobi.h"
 #include "ozaki.h"
 #include "products.h"
+#include "tsqr.h"
 
 namespace hb {
 
@@ -501,9 +502,30 @@ void transpose(const double *src, long long lds, int rows, int cols, double *dst
   }
 }
 
+// Columns j of a block's U and V scaled by a and 1 / a, a = (|V_j| / |U_j|)^(1/2),
+// so both get the norm (|U_j| |V_j|)^(1/2): the product U V^T is unchanged.
+struct BalanceDesc {
+  double *U, *V;
+  int m, n, s;
+  const double *nu2, *nv2;   // squared column norms of U and V
+};
+__global__ void balance_kernel(const BalanceDesc *__restrict__ d) {
+  const BalanceDesc B = d[blockIdx.y];
+  for (int j = blockIdx.x; j < B.s; j += gridDim.x) {
+    const double nu = B.nu2[j], nv = B.nv2[j];
+    if (!(nu > 0.0) || !(nv > 0.0)) continue;
+    const double a = sqrt(sqrt(nv / nu)), ia = 1.0 / a;
+    for (int i = threadIdx.x; i < B.m; i += blockDim.x) B.U[i + (long long)j * B.m] *= a;
+    for (int i = threadIdx.x; i < B.n; i += blockDim.x) B.V[i + (long long)j * B.n] *= ia;
+  }
+}
+
 // H^T as a device tree of the same geometry: leaf i is D_i^T, block (d, j, c)
 // is the transpose of block (d, j, 3 - c) (U and V swapped), so H^T X is an
-// op-N product of this tree.
+// op-N product of this tree.  Its U (the old V, orthonormal columns) and V
+// (the old U, scaled by the singular values) are rebalanced to equal column
+// norms: the int8 rows of the product concatenate a leaf row with U rows and
+// share one exponent, so U entries far below the leaf's would lose bits.
 DeviceTree &transposed_tree(DeviceTree &t, cudaStream_t s) {
   if (t.transposed) return *t.transposed;
   Geometry gt = t.g;
@@ -529,8 +551,36 @@ DeviceTree &transposed_tree(DeviceTree &t, cudaStream_t s) {
   if (!cp.empty()) {
     CopyDesc *d = upload(cp, s);
     copy2d_batched(d, (int)cp.size(), s);
+    // rebalance every block's columns
+    long long tot = 0;
+    std::vector<long long> off(gt.nblock(), 0);
+    for (int b = 0; b < gt.nblock(); ++b) {
+      off[b] = tot;
+      tot += 2LL * tt->g.blocks[b].s;
+    }
+    double *norms = nullptr;
+    HB_CUDA(cudaMalloc((void **)&norms, sizeof(double) * std::max(tot, 1LL)));
+    std::vector<NormDesc> nd;
+    std::vector<BalanceDesc> bd;
+    for (int b = 0; b < gt.nblock(); ++b) {
+      const BlockDesc &B = tt->g.blocks[b];
+      if (B.s == 0) continue;
+      double *U = tt->arena + B.u_off, *V = tt->arena + B.v_off;
+      nd.push_back(NormDesc{U, B.m, B.m, B.s, norms + off[b]});
+      nd.push_back(NormDesc{V, B.n, B.n, B.s, norms + off[b] + B.s});
+      bd.push_back(BalanceDesc{U, V, B.m, B.n, B.s, norms + off[b], norms + off[b] + B.s});
+    }
+    column_norms2(nd, s);
+    BalanceDesc *dbd = upload(bd, s);
+    for (size_t o = 0; o < bd.size(); o += 65535) {
+      balance_kernel<<<dim3(64, (unsigned)std::min<size_t>(65535, bd.size() - o)), 128, 0, s>>>(
+          dbd + o);
+      HB_LAUNCHED();
+    }
     HB_CUDA(cudaStreamSynchronize(s));
     cudaFree(d);
+    cudaFree(dbd);
+    cudaFree(norms);
   }
   t.transposed = tt;
   return *tt;
