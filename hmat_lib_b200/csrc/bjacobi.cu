@@ -8,8 +8,11 @@
 //   1. copy the pair's X columns into its panel and its V columns aside;
 //   2. TSQR of every panel: panel = Q R (Q written over the panel);
 //   3. one-sided Jacobi SVD of every R: R = (U_R Sigma) W^T, sorted;
-//   4. X[:, pair] = Q (U_R Sigma), V[:, pair] = V_old[:, pair] W (batched GEMMs);
-//   5. a pair whose Jacobi rotated anything marks its problem.
+//   4. X[:, pair] = Q (U_R Sigma), V[:, pair] = V_old[:, pair] W, and a pair
+//      whose Jacobi rotated anything marks its problem (one update launch).
+// The TSQR plan and the Jacobi problems of the pair slots are made once per
+// set of active problems; a round only uploads its copy and update
+// descriptors.
 // Round r of a sweep pairs blocks as the round-robin tournament does (block
 // players - 1 fixed, the others rotating), so a sweep of players - 1 rounds
 // pairs every block with every other once.
@@ -19,7 +22,6 @@
 
 #include "bjacobi.h"
 #include "dtree.h"
-#include "gemm_f64.h"
 #include "jacobi.h"
 #include "tsqr.h"
 
@@ -61,12 +63,57 @@ __global__ void bj_identity_kernel(double *__restrict__ v, long long ld, int n) 
     v[i + (long long)i * ld] = 1.0;
 }
 
-// problem owner[k] rotated something in this round when pair slot k's Jacobi
-// needed more than its first (checking) sweep
-__global__ void bj_flag_kernel(const int *__restrict__ sweeps, const int *__restrict__ owner,
-                               int nslots, int *__restrict__ rotated) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nslots; k += gridDim.x * blockDim.x)
-    if (sweeps[k] > 1) rotated[owner[k]] = 1;
+// One pair's update: X[:, a | b] = P (U_R Sigma) with P the pair's Q (L x 32),
+// V[:, a | b] = T W with T the pair's old V columns (Lp x 32); 64 rows and 32
+// columns per CTA (a thread: one row, eight columns), the two 32 x 32 factors
+// in shared memory.  The first CTA of a pair also marks the problem when the
+// pair's Jacobi SVD rotated anything (more than its first, checking sweep).
+struct BjUpdate {
+  const double *P, *T, *JU, *JV;
+  double *xa, *xb, *va, *vb;
+  int L, Lp;
+  const int *sweeps;
+  int *rotated;
+};
+
+__global__ void __launch_bounds__(256) bj_update_kernel(const BjUpdate *__restrict__ ups) {
+  const BjUpdate U = ups[blockIdx.y];
+  __shared__ double ju[kPair * kPair], jv[kPair * kPair];
+  for (int e = threadIdx.x; e < kPair * kPair; e += blockDim.x) {
+    ju[e] = U.JU[e];
+    jv[e] = U.JV[e];
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *U.sweeps > 1) *U.rotated = 1;
+  const int row = blockIdx.x * 64 + (threadIdx.x & 63), g = threadIdx.x >> 6;   // columns 8g..8g+7
+  if (row < U.L) {
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < kPair; ++k) {
+      const double pk = U.P[row + (long long)k * U.L];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = fma(pk, ju[k + (8 * g + c) * kPair], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int col = 8 * g + c;
+      double *dst = col < kBj ? U.xa + (long long)col * U.L : U.xb + (long long)(col - kBj) * U.L;
+      dst[row] = acc[c];
+    }
+  }
+  if (row < U.Lp) {
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < kPair; ++k) {
+      const double tk = U.T[row + (long long)k * U.Lp];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = fma(tk, jv[k + (8 * g + c) * kPair], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int col = 8 * g + c;
+      double *dst = col < kBj ? U.va + (long long)col * U.Lp : U.vb + (long long)(col - kBj) * U.Lp;
+      dst[row] = acc[c];
+    }
+  }
 }
 
 // Blocks (a, b) of pair k in round r of a round-robin over `players` (even).
@@ -132,18 +179,11 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
   for (int p = 0; p < np; ++p) noff[p] = take(wk[p].Lp);
   double *w = dev_alloc(total, s);
   HB_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * total, s));
-  int *d_ints = nullptr;   // per slot: rank, sweeps, owner; per problem: rotated flag
-  HB_CUDA(cudaMallocAsync((void **)&d_ints, sizeof(int) * (3 * nslots + np), s));
-  HB_CUDA(cudaMemsetAsync(d_ints, 0, sizeof(int) * (3 * nslots + np), s));
-  int *d_rank = d_ints, *d_sw = d_ints + nslots, *d_owner = d_ints + 2 * nslots;
-  int *d_rot = d_ints + 3 * nslots;
-  {
-    std::vector<int> owner(nslots);
-    for (int p = 0; p < np; ++p)
-      for (int k = 0; k < wk[p].npairs; ++k) owner[wk[p].slot0 + k] = p;
-    HB_CUDA(cudaMemcpyAsync(d_owner, owner.data(), sizeof(int) * nslots, cudaMemcpyHostToDevice,
-                            s));
-  }
+  int *d_ints = nullptr;   // per slot: rank, sweeps; per problem: rotated flag
+  HB_CUDA(cudaMallocAsync((void **)&d_ints, sizeof(int) * (2 * nslots + np), s));
+  HB_CUDA(cudaMemsetAsync(d_ints, 0, sizeof(int) * (2 * nslots + np), s));
+  int *d_rank = d_ints, *d_sw = d_ints + nslots;
+  int *d_rot = d_ints + 2 * nslots;
   // ---- X = A^T, V = I, thresholds -------------------------------------------------------
   std::vector<NormDesc> nd;
   for (int p = 0; p < np; ++p) {
@@ -170,8 +210,6 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
       wk[p].fro = std::sqrt(f2);
     }
   }
-  GemmBases bases{};
-  for (int i = 0; i < kGemmBases; ++i) bases.p[i] = w;
   JacobiParams prm;
   prm.trunc = Truncation::None;
   prm.scale_u = 1;
@@ -180,16 +218,64 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
   prm.conv_tol = 8.0 * std::sqrt((double)lmax) * 2.220446049250313e-16;
   std::vector<int> rot(np, 0);
 
+  // The TSQR plan and the Jacobi problems cover every pair slot of every
+  // active problem; they depend only on the slots' addresses, so they are
+  // made once per set of active problems.  A slot whose pair is a bye this
+  // round computes on stale values that nothing reads.
+  std::unique_ptr<TsqrPlan, TsqrPlanDeleter> tplan;
+  JacobiProb *d_jp = nullptr;
+  int njp = 0;
+  auto make_plans = [&]() {
+    std::vector<TsqrProb> tq;
+    std::vector<JacobiProb> jp;
+    for (int p = 0; p < np; ++p) {
+      const Work &W = wk[p];
+      if (!W.active) continue;
+      for (int k = 0; k < W.npairs; ++k) {
+        const long long pk = W.pnl + (long long)k * W.L * kPair;
+        const long long rk = W.r + (long long)k * kPair * kPair;
+        tq.push_back(TsqrProb{w + pk, W.L, W.L, kPair, w + rk, kPair});
+        JacobiProb j{};
+        j.A = w + rk;
+        j.lda = kPair;
+        j.transA = 0;
+        j.m = kPair;
+        j.n = kPair;
+        j.G = w + W.jw + (long long)k * jws;
+        j.W = j.G + align_up((long long)kPair * kPair);
+        j.U = w + W.ju + (long long)k * kPair * kPair;
+        j.ldu = kPair;
+        j.V = w + W.jv + (long long)k * kPair * kPair;
+        j.ldv = kPair;
+        j.sigma = w + W.js + (long long)k * kPair;
+        j.rank = d_rank + W.slot0 + k;
+        j.sweeps = d_sw + W.slot0 + k;
+        j.skip_abs = W.theta;
+        // A pair's columns are recomputed every round, so a large and a small
+        // column keep a coupling of about eps ||A|| ||large||; such pairs
+        // count as orthogonal (singular values then carry an absolute error
+        // of that order, far below the truncation threshold tol ||A||),
+        // otherwise sweeps would never end.
+        j.conv_scale = W.fro;
+        jp.push_back(j);
+      }
+    }
+    tplan = tsqr_plan(tq, s);
+    if (d_jp) cudaFreeAsync(d_jp, s);
+    d_jp = upload_vec(jp, s);
+    njp = (int)jp.size();
+  };
+  make_plans();
+  int lpmax = 0;
+  for (const Work &W : wk) lpmax = std::max(lpmax, W.Lp);
+
   // ---- rounds ------------------------------------------------------------------------------
   for (long long guard = 0; guard < 1000000; ++guard) {
     bool any = false;
     for (const Work &W : wk) any = any || W.active;
     if (!any) break;
     std::vector<CopyDesc> cp;
-    std::vector<TsqrProb> tq;
-    std::vector<JacobiProb> jp;
-    GemmBatch gx, gv;
-    HB_CUDA(cudaMemsetAsync(d_sw, 0, sizeof(int) * nslots, s));
+    std::vector<BjUpdate> up;
     for (int p = 0; p < np; ++p) {
       const Work &W = wk[p];
       if (!W.active) continue;
@@ -200,63 +286,30 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
         if (b >= W.nblk) continue;   // the bye of an odd block count
         const long long pk = W.pnl + (long long)k * L * kPair;
         const long long tk = W.tmp + (long long)k * Lp * kPair;
-        const long long rk = W.r + (long long)k * kPair * kPair;
-        const long long uk = W.ju + (long long)k * kPair * kPair;
-        const long long vk = W.jv + (long long)k * kPair * kPair;
-        const long long xa = W.x + (long long)a * kBj * L, xb = W.x + (long long)b * kBj * L;
-        const long long va = W.v + (long long)a * kBj * Lp, vb = W.v + (long long)b * kBj * Lp;
-        cp.push_back(CopyDesc{w + xa, L, w + pk, L, (int)L, kBj});
-        cp.push_back(CopyDesc{w + xb, L, w + pk + kBj * L, L, (int)L, kBj});
-        cp.push_back(CopyDesc{w + va, Lp, w + tk, Lp, (int)Lp, kBj});
-        cp.push_back(CopyDesc{w + vb, Lp, w + tk + kBj * Lp, Lp, (int)Lp, kBj});
-        tq.push_back(TsqrProb{w + pk, L, (int)L, kPair, w + rk, kPair});
-        JacobiProb j{};
-        j.A = w + rk;
-        j.lda = kPair;
-        j.transA = 0;
-        j.m = kPair;
-        j.n = kPair;
-        j.G = w + W.jw + (long long)k * jws;
-        j.W = j.G + align_up((long long)kPair * kPair);
-        j.U = w + uk;
-        j.ldu = kPair;
-        j.V = w + vk;
-        j.ldv = kPair;
-        j.sigma = w + W.js + (long long)k * kPair;
-        j.rank = d_rank + W.slot0 + k;
-        j.sweeps = d_sw + W.slot0 + k;
-        j.skip_abs = W.theta;
-        // A pair's columns are recomputed by a GEMM every round, so a large
-        // and a small column keep a coupling of about eps ||A|| ||large||;
-        // such pairs count as orthogonal (singular values then carry an
-        // absolute error of that order, far below the truncation threshold
-        // tol ||A||), otherwise sweeps would never end.
-        j.conv_scale = W.fro;
-        jp.push_back(j);
-        // X[:, a] = Q (U_R S)[:, 0:16], X[:, b] = Q (U_R S)[:, 16:32]
-        int q = gx.add(0, xa, L, (int)L, kBj);
-        gx.seg(q, 0, pk, L, 0, 0, uk, kPair, 0, kPair);
-        q = gx.add(0, xb, L, (int)L, kBj);
-        gx.seg(q, 0, pk, L, 0, 0, uk + kBj * kPair, kPair, 0, kPair);
-        // V[:, a] = V_old[:, pair] W[:, 0:16], V[:, b] = V_old[:, pair] W[:, 16:32]
-        q = gv.add(0, va, Lp, (int)Lp, kBj);
-        gv.seg(q, 0, tk, Lp, 0, 0, vk, kPair, 0, kPair);
-        q = gv.add(0, vb, Lp, (int)Lp, kBj);
-        gv.seg(q, 0, tk, Lp, 0, 0, vk + kBj * kPair, kPair, 0, kPair);
+        double *xa = w + W.x + (long long)a * kBj * L, *xb = w + W.x + (long long)b * kBj * L;
+        double *va = w + W.v + (long long)a * kBj * Lp, *vb = w + W.v + (long long)b * kBj * Lp;
+        cp.push_back(CopyDesc{xa, L, w + pk, L, (int)L, kBj});
+        cp.push_back(CopyDesc{xb, L, w + pk + kBj * L, L, (int)L, kBj});
+        cp.push_back(CopyDesc{va, Lp, w + tk, Lp, (int)Lp, kBj});
+        cp.push_back(CopyDesc{vb, Lp, w + tk + kBj * Lp, Lp, (int)Lp, kBj});
+        up.push_back(BjUpdate{w + pk, w + tk, w + W.ju + (long long)k * kPair * kPair,
+                              w + W.jv + (long long)k * kPair * kPair, xa, xb, va, vb, (int)L,
+                              (int)Lp, d_sw + W.slot0 + k, d_rot + p});
       }
     }
     if (!cp.empty()) {
       CopyDesc *d = upload_vec(cp, s);
       copy2d_batched(d, (int)cp.size(), s);
       cudaFreeAsync(d, s);
-      tsqr_batched(tq, s);
-      JacobiProb *dj = upload_vec(jp, s);
-      jacobi_svd_batched(dj, (int)jp.size(), prm, d_status, kPair, s);
-      cudaFreeAsync(dj, s);
-      gemm_f64_run(gx, bases, TileShape::M128N64, s, false);
-      gemm_f64_run(gv, bases, TileShape::M128N64, s, false);
-      bj_flag_kernel<<<(nslots + 255) / 256, 256, 0, s>>>(d_sw, d_owner, nslots, d_rot);
-      HB_LAUNCHED();
+      tsqr_run(*tplan, s);
+      jacobi_svd_batched(d_jp, njp, prm, d_status, kPair, s);
+      BjUpdate *du = upload_vec(up, s);
+      for (size_t o = 0; o < up.size(); o += 65535) {
+        dim3 grid((lpmax + 63) / 64, (unsigned)std::min<size_t>(65535, up.size() - o));
+        bj_update_kernel<<<grid, 256, 0, s>>>(du + o);
+        HB_LAUNCHED();
+      }
+      cudaFreeAsync(du, s);
     }
     // end of a sweep: a problem whose sweep rotated nothing has converged
     bool check = false;
@@ -267,6 +320,7 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
     if (!check) continue;
     HB_CUDA(cudaMemcpyAsync(rot.data(), d_rot, sizeof(int) * np, cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
+    bool changed = false;
     for (int p = 0; p < np; ++p) {
       Work &W = wk[p];
       if (!W.active || W.round != W.players - 1) continue;
@@ -275,13 +329,22 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
       if (!rot[p]) {
         W.active = false;
         W.converged = true;
+        changed = true;
       } else if (W.sweep >= max_sweeps) {
         W.active = false;
+        changed = true;
       } else {
         HB_CUDA(cudaMemsetAsync(d_rot + p, 0, sizeof(int), s));
       }
     }
+    if (changed) {
+      bool more = false;
+      for (const Work &W : wk) more = more || W.active;
+      if (more) make_plans();
+    }
   }
+  if (d_jp) cudaFreeAsync(d_jp, s);
+  tplan.reset();
 
   // ---- singular values, order, rank, outputs -------------------------------------------
   nd.clear();

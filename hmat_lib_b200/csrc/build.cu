@@ -185,12 +185,20 @@ std::vector<float> block_features(const std::vector<SketchBlock> &sk,
 const BuildStats &last_build_stats() { return g_last_stats; }
 const std::vector<float> &last_build_features() { return g_last_features; }
 
-std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInput> &in,
-                                                     double tol, cudaStream_t stream,
-                                                     int *svd_status, BuildStats *stats,
-                                                     const KernelSpec *gen) {
-  auto t0 = std::chrono::steady_clock::now();
-  gemm_flops_counter() = 0.0;
+namespace {
+
+// One build attempt.  With `wide` false (and sketch_cap 0) every sketched
+// block first gets a modest width cap -- 1024 columns, or twice its
+// predicted one-shot width -- so that a build whose ranks are small never
+// reserves (and maps) scratch for full-width sketches; the first block that
+// reaches such a cap while its memory-bounded cap is larger abandons the
+// attempt (*retry set, no trees returned), and the caller runs the build
+// again with the memory-bounded caps (`wide` true).
+std::vector<std::shared_ptr<DeviceTree>> build_attempt(
+    const std::vector<BuildInput> &in, double tol, cudaStream_t stream, int *svd_status,
+    BuildStats *stats, const KernelSpec *gen, bool wide, bool *retry,
+    std::chrono::steady_clock::time_point t0) {
+  *retry = false;
   HB_REQUIRE(!in.empty(), INPUT_ERROR, "build: no tree to build");
   HB_REQUIRE(!gen || in.size() == 1, INPUT_ERROR, "a matrix-free build takes one tree");
   *svd_status = SUCCESS;
@@ -390,6 +398,16 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
       }
     }
   }
+  // the first attempt's caps: 1024 columns or twice the one-shot width
+  std::vector<int> memcap(sk.size());
+  for (size_t i = 0; i < sk.size(); ++i) {
+    SketchBlock &S = sk[i];
+    memcap[i] = S.cap;
+    if (!wide && cap_opt <= 0) {
+      const int want = std::max(1024, (2 * S.first_w + kPanel - 1) / kPanel * kPanel);
+      S.cap = std::min(S.cap, want);
+    }
+  }
   // scratch of the sketched blocks: test matrices and products as wide as a
   // block's widest round
   int w_max = std::max(w_first, w_next);
@@ -487,8 +505,10 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
       if (wb[i] <= 0) {
         sk[i].done = true;
         cap_hit = true;
+        if (!wide && sk[i].cap < memcap[i]) *retry = true;
       }
     }
+    if (*retry) break;
     act.erase(std::remove_if(act.begin(), act.end(), [&](int i) { return wb[i] <= 0; }),
               act.end());
     if (act.empty()) break;
@@ -694,6 +714,17 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
     ++rounds;
   }
 
+  if (*retry) {
+    // abandon this attempt: release what it holds, the caller builds again
+    HB_CUDA(cudaStreamSynchronize(stream));
+    for (auto &e : ev) cudaEventDestroy(e);
+    dev_free(d_eprobs, stream);
+    dev_free(d_int, stream);
+    dev_free(work, stream);
+    smix.reset();
+    HB_CUDA(cudaStreamSynchronize(stream));
+    return {};
+  }
   HB_CUDA(cudaEventRecord(ev[2], stream));
 
   // ---- SVD of R_B^T for the sketched blocks ------------------------------------------
@@ -918,6 +949,20 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
   g_last_stats = st;
   if (stats) *stats = st;
   return dts;
+}
+
+}  // namespace
+
+std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInput> &in,
+                                                     double tol, cudaStream_t stream,
+                                                     int *svd_status, BuildStats *stats,
+                                                     const KernelSpec *gen) {
+  const auto t0 = std::chrono::steady_clock::now();
+  gemm_flops_counter() = 0.0;
+  bool retry = false;
+  auto trees = build_attempt(in, tol, stream, svd_status, stats, gen, false, &retry, t0);
+  if (!retry) return trees;
+  return build_attempt(in, tol, stream, svd_status, stats, gen, true, &retry, t0);
 }
 
 std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g, const double *d_A, long long lda,

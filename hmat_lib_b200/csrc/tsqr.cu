@@ -256,8 +256,30 @@ void panel_clean(const std::vector<CleanDesc> &descs, double rel, cudaStream_t s
   cudaFreeAsync(d, s);
 }
 
-void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t s) {
-  if (probs.empty()) return;
+// The chunk lists of every level of a batch of TSQR problems, uploaded, with
+// the scratch of the stacked R factors: made once, run any number of times
+// (the panels' contents may change between runs, not their addresses).
+struct TsqrPlan {
+  std::vector<QrChunk *> up;        // per level: QR of the chunks
+  std::vector<int> up_n;
+  std::vector<MulChunk *> down;     // per level (top first): Q times the parent's Q
+  std::vector<int> down_n;
+  double *buf = nullptr;
+  cudaStream_t stream = nullptr;
+  ~TsqrPlan() {
+    for (auto *p : up) cudaFreeAsync(p, stream);
+    for (auto *p : down) cudaFreeAsync(p, stream);
+    if (buf) cudaFreeAsync(buf, stream);
+  }
+};
+
+void TsqrPlanDeleter::operator()(TsqrPlan *p) const { delete p; }
+
+std::unique_ptr<TsqrPlan, TsqrPlanDeleter> tsqr_plan(const std::vector<TsqrProb> &probs,
+                                                     cudaStream_t s) {
+  std::unique_ptr<TsqrPlan, TsqrPlanDeleter> plan(new TsqrPlan);
+  plan->stream = s;
+  if (probs.empty()) return plan;
   // level structure of every problem: level 0 is the panel itself, level
   // l + 1 stacks the w x w R factors of level l's chunks
   struct Level {
@@ -282,15 +304,14 @@ void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t s) {
       scratch += align_up((long long)rows * P.w);
     }
   }
-  double *buf = nullptr;
-  if (scratch) HB_CUDA(cudaMallocAsync((void **)&buf, scratch * sizeof(double), s));
+  if (scratch) HB_CUDA(cudaMallocAsync((void **)&plan->buf, scratch * sizeof(double), s));
   int max_levels = 0;
   for (size_t p = 0; p < probs.size(); ++p) {
     auto &L = levels[p];
     L[0].A = probs[p].Y;
     L[0].lda = probs[p].ldy;
     for (size_t l = 1; l < L.size(); ++l) {
-      L[l].A = buf + stack_off[p][l - 1];
+      L[l].A = plan->buf + stack_off[p][l - 1];
       L[l].lda = L[l].rows;
     }
     max_levels = std::max(max_levels, (int)L.size());
@@ -318,7 +339,8 @@ void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t s) {
         if (q.rows > 0) chunks.push_back(q);
       }
     }
-    launch_qr(chunks, s);
+    plan->up.push_back(chunks.empty() ? nullptr : upload(chunks, s));
+    plan->up_n.push_back((int)chunks.size());
   }
   // down-sweep: every chunk's Q times its block of the parent's Q
   for (int l = max_levels - 2; l >= 0; --l) {
@@ -338,9 +360,37 @@ void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t s) {
         if (mc.rows > 0) chunks.push_back(mc);
       }
     }
-    launch_mul(chunks, s);
+    plan->down.push_back(chunks.empty() ? nullptr : upload(chunks, s));
+    plan->down_n.push_back((int)chunks.size());
   }
-  if (buf) cudaFreeAsync(buf, s);
+  return plan;
+}
+
+void tsqr_run(const TsqrPlan &plan, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    HB_CUDA(cudaFuncSetAttribute(qr_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kQrSmem));
+    configured = true;
+  }
+  for (size_t l = 0; l < plan.up.size(); ++l)
+    for (int off = 0; off < plan.up_n[l]; off += 65535) {
+      const int cnt = std::min(65535, plan.up_n[l] - off);
+      qr_chunk_kernel<<<cnt, kQT, kQrSmem, s>>>(plan.up[l] + off);
+      HB_LAUNCHED();
+    }
+  for (size_t l = 0; l < plan.down.size(); ++l)
+    for (int off = 0; off < plan.down_n[l]; off += 65535) {
+      const int cnt = std::min(65535, plan.down_n[l] - off);
+      mul_chunk_kernel<<<cnt, kQT, 0, s>>>(plan.down[l] + off);
+      HB_LAUNCHED();
+    }
+}
+
+void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t s) {
+  if (probs.empty()) return;
+  auto plan = tsqr_plan(probs, s);
+  tsqr_run(*plan, s);
 }
 
 void gaussian_fill(const std::vector<RandDesc> &descs, unsigned long long seed, cudaStream_t s) {

@@ -2,6 +2,7 @@
 // with the explicit orthonormal factor written over the input.
 #pragma once
 
+#include <memory>
 #include <vector>
 
 #include "common.h"
@@ -22,6 +23,16 @@ struct TsqrProb {
 // Q R = Y for every problem.  Rank-deficient panels still get an orthonormal
 // Q (Householder), R then has (near-)zero diagonal entries.
 void tsqr_batched(const std::vector<TsqrProb> &probs, cudaStream_t stream);
+
+// The same as a reusable plan: made once for fixed panel and R addresses,
+// run whenever the panels hold new values (one launch per tree level).
+struct TsqrPlan;
+struct TsqrPlanDeleter {
+  void operator()(TsqrPlan *p) const;
+};
+std::unique_ptr<TsqrPlan, TsqrPlanDeleter> tsqr_plan(const std::vector<TsqrProb> &probs,
+                                                     cudaStream_t stream);
+void tsqr_run(const TsqrPlan &plan, cudaStream_t stream);
 
 // Zeroes the columns of a freshly orthonormalised sketch panel whose R
 // diagonal is at rounding level, |R_jj| <= rel * max_c ||Y_c||, where ||Y_c||
