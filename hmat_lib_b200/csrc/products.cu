@@ -100,7 +100,11 @@ long long product_w_layout(const DeviceTree &t, int k, std::vector<long long> &w
   return w_total;
 }
 
+// Tile shape of a product phase: option product_shape1 / product_shape2
+// (0-3: 128x64, 64x128, 32x128, 32x256), else by op and k.
 TileShape default_shape(ProdOp op, int k, int phase) {
+  const int forced = (int)option(phase == 1 ? "product_shape1" : "product_shape2", -1.0);
+  if (forced >= 0 && forced <= 3) return (TileShape)forced;
   if (phase == 1) return (op == ProdOp::L) ? TileShape::M128N64 : TileShape::M64N128;
   return (op == ProdOp::L && k <= 64) ? TileShape::M64N128 : TileShape::M128N64;
 }
@@ -108,7 +112,9 @@ TileShape default_shape(ProdOp op, int k, int phase) {
 ProductPlan &product_plan(DeviceTree &t, ProdOp op, int k, long long ldx, long long ldy,
                           cudaStream_t stream, int min_depth) {
   std::lock_guard<std::mutex> lk(t.plan_mutex);
-  auto key = std::make_tuple((int)op, k, ldx, ldy, (int)Precision::FP64, min_depth);
+  // the tile shapes are part of the key (precision field: FP64 plus the shapes)
+  const int shapes = 16 * (1 + (int)default_shape(op, k, 1)) + 256 * (1 + (int)default_shape(op, k, 2));
+  auto key = std::make_tuple((int)op, k, ldx, ldy, (int)Precision::FP64 + shapes, min_depth);
   auto it = t.plans.find(key);
   if (it != t.plans.end()) return *it->second;
 

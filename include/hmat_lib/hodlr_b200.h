@@ -98,6 +98,9 @@ const char *hodlr_b200_last_error(void);
  *       (hodlr_b200_phase_times)
  *   gemm_f64_engine (1): FP64 products on the FP64 tensor cores (DMMA); 0 =
  *       the DFMA kernel
+ *   product_shape1 (-1), product_shape2 (-1): tile shape of the FP64 product's
+ *       projection / output phase (0: 128x64, 1: 64x128, 2: 32x128,
+ *       3: 32x256; -1: chosen by op and k)
  *   product_graphs (1): a device FP64 product that repeats an earlier call
  *       (same tree, op, sizes, buffers and non-default stream) is captured
  *       once as a CUDA graph and replayed; 0 = always launch directly */
