@@ -22,20 +22,21 @@ struct BjProb {
   int *sweeps;     // out (device int, optional): sweeps used; max_sweeps + 1 if not converged
 };
 
-// Columns of A are taken 16 at a time (blocks); every round pairs each block
-// with another (round-robin over the blocks), and each pair of 32 columns is
-// factored Q R by TSQR, R = U_R Sigma W^T by the one-sided Jacobi SVD, and the
-// pair's columns replaced by Q U_R Sigma while W is applied to the
-// accumulated right rotations: a handful of batched launches per round for
-// all pairs of all problems, so the work is GEMM- and QR-shaped instead of the
-// pairwise rotations of the one-CTA / one-cluster solver, whose every round
-// streams the whole matrix through a few SMs.  A sweep ends when every block
-// met every other; a problem stops once a whole sweep applied no rotation.
-// Pairs of columns whose norm is below 1e-3 tol ||A||_F / L are not rotated
-// (the same rule as the scalar solver, so no kept singular value moves by
-// more than 0.1% of the truncation threshold).  The rank follows hmat_lib's
-// relative rule (src/constructors.c:329-336).  A problem that has not
-// converged after max_sweeps sweeps sets *d_status to SVD_FAILURE.
+// Columns of A are taken 32 at a time (blocks); every round pairs each block
+// with another (round-robin over the blocks), and for each pair of 64 columns
+// one cluster of CTAs forms the pair's Gram matrix on the FP64 tensor cores,
+// diagonalises it by two-sided Jacobi in shared memory and rotates the pair's
+// columns and the accumulated right rotations by its eigenvectors: one launch
+// per round for all pairs of all problems, so every round streams the
+// columns through all SMs instead of the pairwise rotations of the one-CTA /
+// one-cluster solver, which stream the whole matrix through a few SMs.  A
+// sweep ends when every block met every other; a problem stops once a whole
+// sweep applied no rotation.  Pairs of columns whose norm is below
+// 1e-3 tol ||A||_F / L are not rotated (the same rule as the scalar solver, so
+// no kept singular value moves by more than 0.1% of the truncation
+// threshold).  The rank follows hmat_lib's relative rule
+// (src/constructors.c:329-336).  A problem that has not converged after
+// max_sweeps sweeps sets *d_status to SVD_FAILURE.
 // Synchronises with `stream`.
 void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_sweeps,
                       int *d_status, cudaStream_t stream);

@@ -1,6 +1,7 @@
-"""The block Jacobi SVD of wide sketch cores (16-column blocks paired
-round-robin: TSQR of each 32-column pair, Jacobi SVD of its R, GEMM
-updates), checked through the build: with option jacobi_block_min_c lowered
+"""The block Jacobi SVD of wide sketch cores (32-column blocks paired
+round-robin: Gram matrix of each 64-column pair, its eigenvectors by Jacobi
+in shared memory, rotation of the pair's columns), checked through the
+build: with option jacobi_block_min_c lowered
 so that every sketched core takes the block solver, the tree has the same
 ranks (within one, a singular value at the threshold may fall either side)
 and the same accuracy against the dense product as with the one-CTA /
