@@ -187,18 +187,15 @@ const std::vector<float> &last_build_features() { return g_last_features; }
 
 namespace {
 
-// One build attempt.  With `wide` false (and sketch_cap 0) every sketched
-// block first gets a modest width cap -- 1024 columns, or twice its
-// predicted one-shot width -- so that a build whose ranks are small never
-// reserves (and maps) scratch for full-width sketches; the first block that
-// reaches such a cap while its memory-bounded cap is larger abandons the
-// attempt (*retry set, no trees returned), and the caller runs the build
-// again with the memory-bounded caps (`wide` true).
+// The build.  With sketch_cap 0 every sketched block starts with a modest
+// width cap -- 1024 columns, or twice its predicted one-shot width -- so that
+// a build whose ranks are small never reserves (and maps) scratch for
+// full-width sketches; a block that reaches that cap while its
+// memory-bounded cap is larger moves its sketch into scratch of twice the
+// width (up to the memory-bounded cap) and carries on.
 std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     const std::vector<BuildInput> &in, double tol, cudaStream_t stream, int *svd_status,
-    BuildStats *stats, const KernelSpec *gen, bool wide, bool *retry,
-    std::chrono::steady_clock::time_point t0) {
-  *retry = false;
+    BuildStats *stats, const KernelSpec *gen, std::chrono::steady_clock::time_point t0) {
   HB_REQUIRE(!in.empty(), INPUT_ERROR, "build: no tree to build");
   HB_REQUIRE(!gen || in.size() == 1, INPUT_ERROR, "a matrix-free build takes one tree");
   *svd_status = SUCCESS;
@@ -398,12 +395,12 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
       }
     }
   }
-  // the first attempt's caps: 1024 columns or twice the one-shot width
+  // starting caps: 1024 columns or twice the one-shot width (grown on demand)
   std::vector<int> memcap(sk.size());
   for (size_t i = 0; i < sk.size(); ++i) {
     SketchBlock &S = sk[i];
     memcap[i] = S.cap;
-    if (!wide && cap_opt <= 0) {
+    if (cap_opt <= 0) {
       const int want = std::max(1024, (2 * S.first_w + kPanel - 1) / kPanel * kPanel);
       S.cap = std::min(S.cap, want);
     }
@@ -434,6 +431,42 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   bases.p[kWork] = work;
   for (int i = 2; i < kGemmBases; ++i) bases.p[i] = work;
   if (!sk.empty()) HB_CUDA(cudaMemsetAsync(work, 0, scratch * sizeof(double), stream));
+  // A block at its cap whose memory-bounded cap is larger: Q, B^T, P and R_B
+  // (with its first ell columns) and the round buffers sized by the cap move
+  // to a fresh allocation of twice the width, addressed by offsets from
+  // `work` like the rest.
+  std::vector<double *> grown;
+  auto grow = [&](SketchBlock &S, int limit) {
+    const int c2 = std::min(limit, std::max(2 * S.cap, S.cap + kPanel) / kPanel * kPanel);
+    const long long wbw = std::max(S.first_w, w_next);
+    const long long m = S.m, n = S.n, e = S.ell;
+    const long long sq = align_up(m * c2), sb = align_up(n * c2), sr = align_up((long long)c2 * c2),
+                    st = align_up(c2 * wbw), sc = align_up((long long)c2 * kPanel);
+    const long long total = sq + 2 * sb + sr + st + sc;
+    double *g = dev_alloc(total, stream);
+    grown.push_back(g);
+    HB_CUDA(cudaMemsetAsync(g, 0, sizeof(double) * total, stream));
+    const long long base = (long long)(g - work);
+    const long long q = base, bt = q + sq, pp = bt + sb, rb = pp + sb, t = rb + sr, c = t + st;
+    if (e > 0) {
+      HB_CUDA(cudaMemcpyAsync(work + q, work + S.q, sizeof(double) * m * e,
+                              cudaMemcpyDeviceToDevice, stream));
+      HB_CUDA(cudaMemcpyAsync(work + bt, work + S.bt, sizeof(double) * n * e,
+                              cudaMemcpyDeviceToDevice, stream));
+      HB_CUDA(cudaMemcpyAsync(work + pp, work + S.p, sizeof(double) * n * e,
+                              cudaMemcpyDeviceToDevice, stream));
+      HB_CUDA(cudaMemcpy2DAsync(work + rb, sizeof(double) * c2, work + S.rb,
+                                sizeof(double) * S.cap, sizeof(double) * e, (size_t)e,
+                                cudaMemcpyDeviceToDevice, stream));
+    }
+    S.q = q;
+    S.bt = bt;
+    S.p = pp;
+    S.rb = rb;
+    S.t = t;
+    S.c = c;
+    S.cap = c2;
+  };
 
   // ranks of exact blocks, ranks of sketched blocks, status, then the sweeps
   // used by every Jacobi problem in the same order
@@ -501,14 +534,13 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     std::vector<int> wb(sk.size(), 0);
     for (int i : act) {
       const int wr = rounds == 0 ? sk[i].first_w : w_next;
+      if (sk[i].ell >= sk[i].cap && sk[i].cap < memcap[i]) grow(sk[i], memcap[i]);
       wb[i] = std::min(wr, sk[i].cap - sk[i].ell);
       if (wb[i] <= 0) {
         sk[i].done = true;
         cap_hit = true;
-        if (!wide && sk[i].cap < memcap[i]) *retry = true;
       }
     }
-    if (*retry) break;
     act.erase(std::remove_if(act.begin(), act.end(), [&](int i) { return wb[i] <= 0; }),
               act.end());
     if (act.empty()) break;
@@ -714,17 +746,6 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     ++rounds;
   }
 
-  if (*retry) {
-    // abandon this attempt: release what it holds, the caller builds again
-    HB_CUDA(cudaStreamSynchronize(stream));
-    for (auto &e : ev) cudaEventDestroy(e);
-    dev_free(d_eprobs, stream);
-    dev_free(d_int, stream);
-    dev_free(work, stream);
-    smix.reset();
-    HB_CUDA(cudaStreamSynchronize(stream));
-    return {};
-  }
   HB_CUDA(cudaEventRecord(ev[2], stream));
 
   // ---- SVD of R_B^T for the sketched blocks ------------------------------------------
@@ -895,6 +916,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   dev_free(d_int, stream);
   dev_free(jwork, stream);
   dev_free(work, stream);
+  for (double *g : grown) dev_free(g, stream);
   HB_CUDA(cudaStreamSynchronize(stream));
   if (smix && smix->status(stream) != SUCCESS) {
     *svd_status = SVD_FAILURE;
@@ -959,10 +981,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
                                                      const KernelSpec *gen) {
   const auto t0 = std::chrono::steady_clock::now();
   gemm_flops_counter() = 0.0;
-  bool retry = false;
-  auto trees = build_attempt(in, tol, stream, svd_status, stats, gen, false, &retry, t0);
-  if (!retry) return trees;
-  return build_attempt(in, tol, stream, svd_status, stats, gen, true, &retry, t0);
+  return build_attempt(in, tol, stream, svd_status, stats, gen, t0);
 }
 
 std::shared_ptr<DeviceTree> build_from_dense(const Geometry &g, const double *d_A, long long lda,

@@ -103,7 +103,8 @@ long long product_w_layout(const DeviceTree &t, int k, std::vector<long long> &w
 // Tile shape of a product phase: option product_shape1 / product_shape2
 // (0-3: 128x64, 64x128, 32x128, 32x256), else by op and k.
 TileShape default_shape(ProdOp op, int k, int phase) {
-  const int forced = (int)option(phase == 1 ? "product_shape1" : "product_shape2", -1.0);
+  const int forced =
+      (int)(phase == 1 ? option("product_shape1", -1.0) : option("product_shape2", -1.0));
   if (forced >= 0 && forced <= 3) return (TileShape)forced;
   if (phase == 1) return (op == ProdOp::L) ? TileShape::M128N64 : TileShape::M64N128;
   return (op == ProdOp::L && k <= 64) ? TileShape::M64N128 : TileShape::M128N64;
