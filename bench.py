@@ -491,13 +491,26 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, r
         del a
     torch.cuda.empty_cache()
     # the same trees built in batches (hodlr_b200_build_batched_dev): groups of
-    # up to 64 trees, each group's inputs generated first, then one batched
-    # build per group (the timed part); ranks compared with the per-tree builds
+    # consecutive trees whose dense inputs take at most 40 GB together, each
+    # group's inputs generated first, then one batched build per group (the
+    # timed part); ranks compared with the per-tree builds
     batched_s, rank_mismatch = 0.0, 0
-    group = 64
+    groups, cur, cur_b = [], [], 0
+    for i, it in enumerate(inst):
+        b = 8 * it["n"] * it["n"]
+        if cur and cur_b + b > 40e9:
+            groups.append(cur)
+            cur, cur_b = [], 0
+        cur.append(i)
+        cur_b += b
+    if cur:
+        groups.append(cur)
+    group = max(len(g) for g in groups)
+    batched_stages = {}
     with torch.cuda.stream(stream):
-        for g0 in range(0, len(inst), group):
-            grp = inst[g0:g0 + group]
+        for gi in groups:
+            g0 = gi[0]
+            grp = [inst[i] for i in gi]
             mats = []
             for it in grp:
                 n = it["n"]
@@ -515,6 +528,11 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, r
                                           1e-8, stream=sh)
             stream.synchronize()
             batched_s += time.perf_counter() - t0
+            bst = build_stats(lib)
+            for key in ("ms_small_svd", "ms_rounds", "ms_core_svd", "ms_finish"):
+                batched_stages[key] = batched_stages.get(key, 0.0) + bst[key]
+            batched_stages["sketch_rounds"] = max(batched_stages.get("sketch_rounds", 0),
+                                                  bst["sketch_rounds"])
             for j, t in enumerate(bt):
                 rank_mismatch += int(np.any(t.ranks() != trees[g0 + j].ranks()))
                 t.free()
@@ -567,7 +585,9 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, r
            "sizes": sorted(set(ns)), "k_range": [min(ks), max(ks)],
            "kernel": "exp(-|x-y|/l), l ~ U[0.05,0.5], sorted 1D points, seed 2",
            "build_s_total": build_s,
-           "build_batched": {"seconds": batched_s, "group": group,
+           "build_batched": {"seconds": batched_s, "calls": len(groups), "largest_call": group,
+                             "grouping": "consecutive trees, dense inputs <= 40 GB per call",
+                             "stages_summed_over_calls": batched_stages,
                              "speedup_vs_per_tree": build_s / max(batched_s, 1e-9),
                              "trees_with_other_ranks": rank_mismatch,
                              "entry": "hodlr_b200_build_batched_dev"},

@@ -96,10 +96,21 @@ def main():
     ap.add_argument("--max-minutes", type=float, default=25.0,
                     help="stop drawing new matrices after this long")
     ap.add_argument("--out", default=RM.MODEL_FILE)
+    ap.add_argument("--save-data", default=None,
+                    help="also write the collected rows and their draw indices (.npz)")
+    ap.add_argument("--from-data", default=None,
+                    help="train on rows saved by --save-data instead of drawing")
     args = ap.parse_args()
 
-    specs = draws(args.draws, args.seed)
-    data, owner, skipped, used, secs = collect(specs, args.max_minutes * 60.0)
+    if args.from_data:
+        z = np.load(args.from_data)
+        data, owner = z["data"], z["owner"]
+        skipped, used, secs = int(z["skipped"]), int(z["used"]), float(z["secs"])
+    else:
+        specs = draws(args.draws, args.seed)
+        data, owner, skipped, used, secs = collect(specs, args.max_minutes * 60.0)
+    if args.save_data:
+        np.savez(args.save_data, data=data, owner=owner, skipped=skipped, used=used, secs=secs)
     x, target, rank_fro = data[:, :8], RM.targets_of_ranks(data[:, 13]), data[:, 13]
     drawn = np.unique(owner)
     cut = drawn[int(0.9 * len(drawn))] if len(drawn) > 1 else np.inf
