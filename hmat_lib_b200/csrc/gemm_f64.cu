@@ -36,6 +36,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// bases.p[i] for a runtime i without copying the launch argument array to
+// local memory (a chain of selects on the constant-bank values)
+__device__ __forceinline__ double *base_ptr(const GemmBases &b, int i) {
+  static_assert(kGemmBases == 6, "base_ptr selects among six slots");
+  double *p = b.p[0];
+  p = i == 1 ? b.p[1] : p;
+  p = i == 2 ? b.p[2] : p;
+  p = i == 3 ? b.p[3] : p;
+  p = i == 4 ? b.p[4] : p;
+  p = i == 5 ? b.p[5] : p;
+  return p;
+}
+
 struct KIter {
   int si;      // segment index (absolute)
   int kk;      // position inside the segment
@@ -111,8 +124,8 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
   auto load = [&](int buf, const KIter &it) {
     const GemmSeg S = segs[it.si];
     const bool ga = S.abase == kGenSlot, gb = S.bbase == kGenSlot;
-    const double *A = ga ? nullptr : bases.p[S.abase];
-    const double *B = gb ? nullptr : bases.p[S.bbase];
+    const double *A = ga ? nullptr : base_ptr(bases, S.abase);
+    const double *B = gb ? nullptr : base_ptr(bases, S.bbase);
     double *as = As + buf * kBK * LDA;
     double *bs = Bs + buf * kBK * LDB;
     const int kk = it.kk, kend = it.le;
@@ -198,7 +211,7 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
   }
   cp_async_wait<0>();
 
-  double *C = bases.p[P.cbase] + P.c_off;
+  double *C = base_ptr(bases, P.cbase) + P.c_off;
 #pragma unroll
   for (int i = 0; i < TM; ++i) {
     const int m = tile.m0 + 2 * ty + 32 * (i >> 1) + (i & 1);
@@ -231,13 +244,13 @@ gemm_f64_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ p
 // operands, the first K index) are even, else 8; elements past M, N or the K
 // range are zero-filled.  The ring is as deep as two CTAs per SM allow (2 to
 // 4 stages).
-template <int BM, int BN>
+template <int BM, int BN, int BK>
 struct MmaSmem {
   static constexpr int LDKM = BM + 4;      // [k][m] layout
   static constexpr int LDKN = BN + 4;      // [k][n] layout
-  static constexpr int LDK = kBK + 4;      // [m][k] / [n][k] layout
-  static constexpr int A_ELEMS = (kBK * LDKM > BM * LDK) ? kBK * LDKM : BM * LDK;
-  static constexpr int B_ELEMS = (kBK * LDKN > BN * LDK) ? kBK * LDKN : BN * LDK;
+  static constexpr int LDK = BK + 4;      // [m][k] / [n][k] layout
+  static constexpr int A_ELEMS = (BK * LDKM > BM * LDK) ? BK * LDKM : BM * LDK;
+  static constexpr int B_ELEMS = (BK * LDKN > BN * LDK) ? BK * LDKN : BN * LDK;
   static constexpr int STAGE = A_ELEMS + B_ELEMS;
   static constexpr int STAGES_FIT = (int)(112 * 1024 / (sizeof(double) * STAGE));
   static constexpr int STAGES = STAGES_FIT > 4 ? 4 : (STAGES_FIT < 2 ? 2 : STAGES_FIT);
@@ -256,11 +269,11 @@ __device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-template <int BM, int BN, int WM, int WN>
+template <int BM, int BN, int WM, int WN, int BK>
 __global__ void __launch_bounds__(kThreads, 2)
 gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict__ probs,
                     const GemmTile *__restrict__ tiles, GemmBases bases) {
-  using SM = MmaSmem<BM, BN>;
+  using SM = MmaSmem<BM, BN, BK>;
   constexpr int kMmaStages = SM::STAGES;
   constexpr int MT = WM / 8, NT = WN / 8;          // MMA tiles per warp
   constexpr int WARPS_N = BN / WN;
@@ -295,7 +308,7 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
     }
   };
   auto advance = [&](KIter &it) {
-    it.kk += kBK;
+    it.kk += BK;
     if (it.kk >= it.le) {
       it.kbase += segs[it.si].K;
       ++it.si;
@@ -303,7 +316,7 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
     }
   };
 
-  // One operand tile of `rows` lines (M or N side) x kBK into stage memory.
+  // One operand tile of `rows` lines (M or N side) x BK into stage memory.
   // `kcontig`: K is the contiguous dimension in global memory (stored
   // [line][k] in shared memory), otherwise lines are ([k][line]).  Element
   // (line, k) of the tile is global (row0 + line, kk + k) of the operand,
@@ -314,11 +327,11 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
     if (gen) {
       // generated kernel-matrix entries: (r, c) of the block at gen_offset(row0, col0)
       const int gr0 = (int)(off >> 32), gc0 = (int)(off & 0xffffffffLL);
-      for (int e = tid; e < rows * kBK; e += kThreads) {
+      for (int e = tid; e < rows * BK; e += kThreads) {
         int line, k;
         if (kcontig) {
-          line = e / kBK;
-          k = e % kBK;
+          line = e / BK;
+          k = e % BK;
         } else {
           k = e / rows;
           line = e % rows;
@@ -342,8 +355,8 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
     const bool vec = ((off | ld | (kcontig ? kk : 0)) & 1) == 0 &&
                      (((unsigned long long)base) & 15) == 0;
     if (kcontig) {
-      // per line kBK contiguous K values: kBK / 2 chunks of 16 bytes
-      constexpr int CH = kBK / 2;
+      // per line BK contiguous K values: BK / 2 chunks of 16 bytes
+      constexpr int CH = BK / 2;
       for (int e = tid; e < rows * CH; e += kThreads) {
         const int line = e / CH, k = 2 * (e % CH);
         const bool lok = (row0 + line) < nlines;
@@ -360,7 +373,7 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
     } else {
       // per k, `rows` contiguous lines: rows / 2 chunks of 16 bytes
       const int CH = rows / 2;
-      for (int e = tid; e < kBK * CH; e += kThreads) {
+      for (int e = tid; e < BK * CH; e += kThreads) {
         const int k = e / CH, line = 2 * (e % CH);
         const bool kok = (kk + k) < kend;
         const int nl = kok ? min(2, max(0, nlines - (row0 + line))) : 0;
@@ -385,11 +398,11 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
     double *bs = as + SM::A_ELEMS;
     // op(A) is M x K: ta = 0 stores (m, k) at m + k lda (lines contiguous),
     // ta = 1 stores it at k + m lda (K contiguous)
-    load_operand(as, ga, ga ? nullptr : bases.p[S.abase], S.a_off, S.lda, S.ta == 1, BM,
+    load_operand(as, ga, ga ? nullptr : base_ptr(bases, S.abase), S.a_off, S.lda, S.ta == 1, BM,
                  tile.m0, P.M, it.kk, it.le);
     // op(B) is K x N: tb = 0 stores (k, n) at k + n ldb (K contiguous),
     // tb = 1 at n + k ldb (lines contiguous)
-    load_operand(bs, gb, gb ? nullptr : bases.p[S.bbase], S.b_off, S.ldb, S.tb == 0, BN,
+    load_operand(bs, gb, gb ? nullptr : base_ptr(bases, S.bbase), S.b_off, S.ldb, S.tb == 0, BN,
                  tile.n0, P.N, it.kk, it.le);
     return (S.ta == 1 ? 1 : 0) | (S.tb == 0 ? 2 : 0);
   };
@@ -431,7 +444,7 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
     const double *ap = as + (wm0 + g) * a_line_step + t * a_k_step;
     const double *bp = bs + (wn0 + g) * b_line_step + t * b_k_step;
 #pragma unroll
-    for (int k4 = 0; k4 < kBK / 4; ++k4) {
+    for (int k4 = 0; k4 < BK / 4; ++k4) {
       double a[MT], b[NT];
 #pragma unroll
       for (int i = 0; i < MT; ++i) a[i] = ap[(8 * i) * a_line_step + 4 * k4 * a_k_step];
@@ -447,7 +460,7 @@ gemm_f64_mma_kernel(const GemmSeg *__restrict__ segs, const GemmProb *__restrict
   }
   cp_async_wait<0>();
 
-  double *C = bases.p[P.cbase] + P.c_off;
+  double *C = base_ptr(bases, P.cbase) + P.c_off;
 #pragma unroll
   for (int i = 0; i < MT; ++i) {
     const int m = tile.m0 + wm0 + 8 * i + g;
@@ -475,7 +488,7 @@ __global__ void gemm_scale_c_kernel(const GemmProb *__restrict__ probs, int npro
   for (int p = blockIdx.y; p < nprobs; p += gridDim.y) {
     const GemmProb P = probs[p];
     if (P.split <= 1) continue;
-    double *C = bases.p[P.cbase] + P.c_off;
+    double *C = base_ptr(bases, P.cbase) + P.c_off;
     const long long total = (long long)P.M * P.N;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
@@ -488,15 +501,29 @@ __global__ void gemm_scale_c_kernel(const GemmProb *__restrict__ probs, int npro
 
 template <int BM, int BN, int WM, int WN>
 void launch_gemm(const GemmPlan &plan, const GemmBases &bases, cudaStream_t stream) {
-  if (gemm_f64_engine() == 1) {
+  const int engine = gemm_f64_engine();
+  if (engine == 1) {
     static bool configured = false;
-    const size_t smem = MmaSmem<BM, BN>::bytes;
+    const size_t smem = MmaSmem<BM, BN, 16>::bytes;
     if (!configured) {
-      HB_CUDA(cudaFuncSetAttribute(gemm_f64_mma_kernel<BM, BN, WM, WN>,
+      HB_CUDA(cudaFuncSetAttribute(gemm_f64_mma_kernel<BM, BN, WM, WN, 16>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       configured = true;
     }
-    gemm_f64_mma_kernel<BM, BN, WM, WN><<<plan.ntiles, kThreads, smem, stream>>>(
+    gemm_f64_mma_kernel<BM, BN, WM, WN, 16><<<plan.ntiles, kThreads, smem, stream>>>(
+        plan.segs, plan.probs, plan.tiles, bases);
+    HB_LAUNCHED();
+    return;
+  }
+  if (engine == 2) {
+    static bool configured = false;
+    const size_t smem = MmaSmem<BM, BN, 32>::bytes;
+    if (!configured) {
+      HB_CUDA(cudaFuncSetAttribute(gemm_f64_mma_kernel<BM, BN, WM, WN, 32>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured = true;
+    }
+    gemm_f64_mma_kernel<BM, BN, WM, WN, 32><<<plan.ntiles, kThreads, smem, stream>>>(
         plan.segs, plan.probs, plan.tiles, bases);
     HB_LAUNCHED();
     return;
