@@ -36,7 +36,7 @@ enum HodlrB200Op {
 enum { HODLR_B200_CUDA_ERROR = 100 };
 
 enum HodlrB200Precision {
-  HODLR_B200_FP64 = 0,   /* FP64 DFMA products */
+  HODLR_B200_FP64 = 0,   /* FP64 products (FP64 tensor cores) */
   HODLR_B200_MIXED = 1   /* split-precision tensor-core products with FP64 result */
 };
 
@@ -80,7 +80,8 @@ const char *hodlr_b200_last_error(void);
  *   jacobi_cluster_min_c (192): problems this wide or wider use a cluster of
  *       8 CTAs
  *   jacobi_block_min_c (1024): sketch cores this wide or wider are solved by
- *       the block Jacobi SVD (16-column blocks, QR + small SVD + GEMM rounds)
+ *       the block Jacobi SVD (32-column blocks; per round one launch: Gram of
+ *       each 64-column pair, its eigenvectors, in-place rotation)
  *   hxh_dense_max (256): H x H blocks up to this many rows are recompressed
  *       from their dense product
  *   hxh_precision (0): 1 = the subtree products of H x H on the int8 tensor
@@ -96,8 +97,9 @@ const char *hodlr_b200_last_error(void);
  *   ozaki_copy_split (1): bulk copies per int8 operand block
  *   record_phase_times (0): events around each product phase and its main GEMM
  *       (hodlr_b200_phase_times)
- *   gemm_f64_engine (1): FP64 products on the FP64 tensor cores (DMMA); 0 =
- *       the DFMA kernel
+ *   gemm_f64_engine (1): FP64 products on the FP64 tensor cores (DMMA) with
+ *       16-deep K stages; 2 = the same with 32-deep K stages; 0 = the DFMA
+ *       kernel
  *   product_shape1 (-1), product_shape2 (-1): tile shape of the FP64 product's
  *       projection / output phase (0: 128x64, 1: 64x128, 2: 32x128,
  *       3: 32x256; -1: chosen by op and k)
