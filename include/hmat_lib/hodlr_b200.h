@@ -97,8 +97,8 @@ const char *hodlr_b200_last_error(void);
  *   ozaki_copy_split (1): bulk copies per int8 operand block
  *   record_phase_times (0): events around each product phase and its main GEMM
  *       (hodlr_b200_phase_times)
- *   gemm_f64_engine (1): FP64 products on the FP64 tensor cores (DMMA) with
- *       16-deep K stages; 2 = the same with 32-deep K stages; 0 = the DFMA
+ *   gemm_f64_engine (2): FP64 products on the FP64 tensor cores (DMMA) with
+ *       32-deep K stages; 1 = the same with 16-deep K stages; 0 = the DFMA
  *       kernel
  *   product_shape1 (-1), product_shape2 (-1): tile shape of the FP64 product's
  *       projection / output phase (0: 128x64, 1: 64x128, 2: 32x128,
