@@ -429,6 +429,48 @@ def exp3d_workload(lib, torch, dev, stream, steps, warmup, peak64=None):
         t.matmat(x.data_ptr(), k, n, yy.data_ptr(), n, stream=sh, precision=prec)
         stream.synchronize()
         errs[name] = (torch.linalg.norm(yy[:cols] - yd) / torch.linalg.norm(yd)).item()
+    tree_l.free()
+
+    # dense input (the 34 GB matrix generated on the device, as hmat_lib's
+    # dense_to_tree_hodlr takes it): the plain FP64 build, and the learned build
+    # with its sketch products on the int8 tensor cores
+    dense = {}
+    a = torch.empty(n * n, dtype=torch.float64, device=dev)
+    assert lib.hodlr_b200_kernel_matrix_dev(C.c_void_p(d_pts.data_ptr()), n, 3, 2, w["length"],
+                                            w["diag"], C.c_void_p(a.data_ptr()), n,
+                                            C.c_void_p(sh)) == 0
+    stream.synchronize()
+    for name, opts in (("plain_fp64", {}),
+                       ("learned_mixed", {b"learned_ranks": 1.0, b"build_precision": 1.0,
+                                          b"kernel_length": w["length"]})):
+        for key, v in opts.items():
+            lib.hodlr_b200_set_option(key, v)
+        try:
+            with torch.cuda.stream(stream):
+                stream.synchronize()
+                torch.cuda.nvtx.range_push("build_exp3d_dense_" + name)
+                t0 = time.perf_counter()
+                td = DeviceTree.build(a.data_ptr(), n, n, h, tol, stream=sh)
+                stream.synchronize()
+                sec = time.perf_counter() - t0
+                torch.cuda.nvtx.range_pop()
+        finally:
+            for key in opts:
+                lib.hodlr_b200_set_option(key, 0.0)
+        st = build_stats(lib)
+        yy = torch.zeros(k, n, dtype=torch.float64, device=dev)
+        td.matmat(x.data_ptr(), k, n, yy.data_ptr(), n, stream=sh)
+        stream.synchronize()
+        dense[name] = dict(seconds=sec, max_rank_diff_vs_matrix_free=int(np.max(np.abs(
+                               td.ranks() - ranks))),
+                           rel_err_vs_dense=(torch.linalg.norm(yy[:cols] - yd) /
+                                             torch.linalg.norm(yd)).item(), **st)
+        td.free()
+        del yy
+    del a
+    torch.cuda.empty_cache()
+    dense["speedup_learned_mixed_vs_plain_fp64"] = (dense["plain_fp64"]["seconds"] /
+                                                    dense["learned_mixed"]["seconds"])
     out.update({
         "build": {"plain": dict(seconds=plain_s, **plain_st),
                   "learned": dict(seconds=learned_s, **learned_st,
@@ -442,9 +484,9 @@ def exp3d_workload(lib, torch, dev, stream, steps, warmup, peak64=None):
         "matmat": {"fp64": r64, "mixed": rmx, "bytes_per_step": bytes_step,
                    "speedup_mixed_vs_fp64": r64["ms_per_step"] / rmx["ms_per_step"]},
         "rel_err_vs_dense": errs,
+        "build_dense_input": dense,
         "check": "H X vs A X on 16 of the 128 columns, A generated on the device"})
     tree.free()
-    tree_l.free()
     del x, y, yd
     torch.cuda.empty_cache()
     return out
@@ -747,6 +789,29 @@ def main():
     learned_stats = build_stats(lib)
     ranks_l = tree_l.ranks()
 
+    # ---- learned + mixed build: one-shot sketches and their products (Y = A Omega,
+    # B^T = A^T Q) on the int8 tensor cores (option build_precision) ----------------
+    lib.hodlr_b200_set_option(b"learned_ranks", 1.0)
+    lib.hodlr_b200_set_option(b"kernel_length", w["length"])
+    lib.hodlr_b200_set_option(b"build_precision", 1.0)
+    try:
+        with torch.cuda.stream(stream):
+            stream.synchronize()
+            DeviceTree.build(a.data_ptr(), n, n, h, tol, stream=sh).free()   # warm-up
+            stream.synchronize()
+            torch.cuda.nvtx.range_push("build_learned_mixed")
+            t0 = time.perf_counter()
+            tree_lm = DeviceTree.build(a.data_ptr(), n, n, h, tol, stream=sh)
+            stream.synchronize()
+            build_s_lm = time.perf_counter() - t0
+            torch.cuda.nvtx.range_pop()
+    finally:
+        lib.hodlr_b200_set_option(b"learned_ranks", 0.0)
+        lib.hodlr_b200_set_option(b"kernel_length", 0.0)
+        lib.hodlr_b200_set_option(b"build_precision", 0.0)
+    lm_stats = build_stats(lib)
+    ranks_lm = tree_lm.ranks()
+
     # ---- accuracy against the dense FP64 product (checker: cuBLAS on A) ------------
     x = torch.randn(k, n, dtype=torch.float64, device=dev)      # column-major n x k
     y = torch.zeros(k, n, dtype=torch.float64, device=dev)
@@ -759,8 +824,13 @@ def main():
     tree_l.matmat(x.data_ptr(), k, n, y_l.data_ptr(), n, stream=sh)
     stream.synchronize()
     rel_err_learned = (torch.linalg.norm(y_l - y_dense) / torch.linalg.norm(y_dense)).item()
+    y_l.zero_()
+    tree_lm.matmat(x.data_ptr(), k, n, y_l.data_ptr(), n, stream=sh)
+    stream.synchronize()
+    rel_err_lm = (torch.linalg.norm(y_l - y_dense) / torch.linalg.norm(y_dense)).item()
     del y_l
     tree_l.free()
+    tree_lm.free()
     del a, a_mat, y_dense
     torch.cuda.empty_cache()
 
@@ -997,6 +1067,11 @@ def main():
                                   first_build_in_process_s=build_s_learned_first,
                                   max_rank_diff_vs_plain=int(np.max(np.abs(ranks_l - ranks))),
                                   **learned_stats),
+                  "learned_mixed": dict(seconds=build_s_lm, rel_err_vs_dense=rel_err_lm,
+                                        max_rank_diff_vs_plain=int(np.max(np.abs(ranks_lm - ranks))),
+                                        options="learned_ranks=1, build_precision=1",
+                                        **lm_stats),
+                  "speedup_learned_mixed_vs_plain": build_s / build_s_lm,
                   "matrix_free": dict(seconds=build_s_mf, max_rank_diff_vs_plain=mf_rank_diff,
                                       input="points only (hodlr_b200_build_kernel_dev)",
                                       **mf_stats),
