@@ -750,9 +750,9 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
 
   // ---- SVD of R_B^T for the sketched blocks ------------------------------------------
   // Cores of at least jacobi_block_min_c columns go to the block Jacobi solver
-  // (GEMM- and QR-shaped rounds over all SMs); the others to the one-CTA /
-  // one-cluster solver.
-  const int bj_min = (int)option("jacobi_block_min_c", 1024);
+  // (one launch per round over the pairs of every core, on all SMs); the
+  // others to the one-CTA / one-cluster solver.
+  const int bj_min = (int)option("jacobi_block_min_c", 128);
   std::vector<JacobiProb> sprobs;
   std::vector<long long> s_u(sk.size()), s_v(sk.size());
   int max_l = 0;

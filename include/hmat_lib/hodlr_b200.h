@@ -79,7 +79,7 @@ const char *hodlr_b200_last_error(void);
  *   jacobi_max_sweeps (60): Jacobi sweep bound (SVD_FAILURE past it)
  *   jacobi_cluster_min_c (192): problems this wide or wider use a cluster of
  *       8 CTAs
- *   jacobi_block_min_c (1024): sketch cores this wide or wider are solved by
+ *   jacobi_block_min_c (128): sketch cores this wide or wider are solved by
  *       the block Jacobi SVD (32-column blocks; per round one launch: Gram of
  *       each 64-column pair, its eigenvectors, in-place rotation)
  *   hxh_dense_max (256): H x H blocks up to this many rows are recompressed

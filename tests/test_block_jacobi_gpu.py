@@ -29,7 +29,7 @@ def _build(a, n, h, tol, block_min):
     try:
         return DeviceTree.build(a.data_ptr(), n, n, h, tol)
     finally:
-        lib.hodlr_b200_set_option(b"jacobi_block_min_c", 1024.0)
+        lib.hodlr_b200_set_option(b"jacobi_block_min_c", 128.0)
 
 
 @pytest.mark.parametrize("n,h,kind,length", [(4096, 5, "matern32", 0.1),
@@ -74,7 +74,7 @@ def test_block_solver_against_reference_ranks():
     try:
         t = DeviceTree.build_kernel(d_pts.data_ptr(), n, 3, 2, 0.15, 1e-2, h, meta["tol"])
     finally:
-        lib.hodlr_b200_set_option(b"jacobi_block_min_c", 1024.0)
+        lib.hodlr_b200_set_option(b"jacobi_block_min_c", 128.0)
     assert int(np.abs(t.ranks() - ref["ranks"]).max()) <= 1
     x = W.rhs(n, meta["x_cols"], seed=meta["x_seed"])
     xd = torch.from_numpy(np.ascontiguousarray(x.T)).cuda()
