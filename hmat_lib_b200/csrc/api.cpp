@@ -234,9 +234,10 @@ int dense_to_tree_hodlr(TreeHODLR *hodlr, const int m, const int *ms, double *ma
     register_device_tree(hodlr, dt);
     if (status != SUCCESS) {
       *ierr = status;
-      const BuildStats &st = last_build_stats();
-      set_last_error(st.cap_hit ? "a block's rank reached the sketch cap (option sketch_cap)"
-                                : "Jacobi SVD did not converge within the sweep limit");
+      // a sketch that reached its cap keeps the build's own message (which
+      // cap, and the memory it saw)
+      if (!last_build_stats().cap_hit)
+        set_last_error("Jacobi SVD did not converge within the sweep limit");
       return 1;
     }
     return 0;

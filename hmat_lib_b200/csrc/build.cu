@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <string>
 
 #include "bjacobi.h"
 #include "build.h"
@@ -63,6 +64,26 @@ struct SketchBlock {
   bool fell_back = false;
   int mix = -1;          // index in the int8 sketch products (-1: FP64 GEMMs)
 };
+
+// Device memory free or held unused by the device's default stream-ordered
+// pool (bytes).
+double device_avail_bytes() {
+  size_t free_b = 0, total_b = 0;
+  HB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  double avail = (double)free_b;
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
+            cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        reserved > used)
+      avail += (double)(reserved - used);
+  }
+  (void)cudaGetLastError();
+  return avail;
+}
 
 thread_local BuildStats g_last_stats;
 thread_local std::vector<float> g_last_features;
@@ -281,64 +302,15 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     if (!mb.empty()) smix = std::make_unique<SketchMixed>(mb, stream);
   }
   // Sketch width caps.  Option sketch_cap > 0 fixes one cap for every block;
-  // 0 (default) bounds them by memory: blocks of up to 2048 columns may grow
-  // to their full width, wider ones to alpha min(m, n) columns (whole panels,
-  // at least 2048), with alpha in (0, 1] the largest value whose scratch --
-  // Q, B^T, P, R_B and the round buffers, plus the SVD of the core -- fits
-  // option sketch_mem_frac (default 0.6) of the device memory that is free
-  // or held unused by the stream-ordered pool.
+  // 0 (default): a block may grow to its full width, as long as each growth
+  // of its scratch (and the core SVD that will follow) fits option
+  // sketch_mem_frac (default 0.6) of the device memory that is free or held
+  // unused by the stream-ordered pool at that moment (see grow()).
   std::vector<int> caps(sketched.size(), 0);
-  {
-    const int w_round = std::max(w_first, w_next);
-    // blocks up to kFullCap columns always get their whole width (their
-    // scratch is small); alpha applies to the wider ones
-    constexpr int kFullCap = 2048;
-    auto cap_of = [&](const BlockDesc &B, double alpha) {
-      const int C = std::min(B.m, B.n);
-      if (cap_opt > 0) return std::min(C, std::max(cap_opt, kPanel));
-      if (C <= kFullCap) return C;
-      const int c = (int)std::ceil(alpha * C / kPanel) * kPanel;
-      return std::min(C, std::max(c, kFullCap));
-    };
-    auto bytes_of = [&](double alpha) {
-      double total = 0.0;
-      for (int b : sketched) {
-        const BlockDesc &B = blk[b].B;
-        const double c = cap_of(B, alpha);
-        // q, bt, p, rb, om, t, c, rn, and the core SVD's G, W, U, V
-        total += 8.0 * ((double)B.m * c + 2.0 * B.n * c + c * c + (double)B.n * w_round +
-                        c * w_round + c * kPanel + 2.0 * kPanel * kPanel + 4.0 * c * c);
-      }
-      return total;
-    };
-    double alpha = 1.0;
-    if (cap_opt <= 0) {
-      size_t free_b = 0, total_b = 0;
-      HB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-      double avail = (double)free_b;
-      int dev = 0;
-      cudaMemPool_t pool;
-      if (cudaGetDevice(&dev) == cudaSuccess &&
-          cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t reserved = 0, used = 0;
-        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
-                cudaSuccess &&
-            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
-            reserved > used)
-          avail += (double)(reserved - used);
-      }
-      (void)cudaGetLastError();
-      const double budget = option("sketch_mem_frac", 0.6) * avail;
-      if (bytes_of(1.0) > budget) {
-        double lo = 0.0, hi = 1.0;
-        for (int it = 0; it < 40; ++it) {
-          const double mid = 0.5 * (lo + hi);
-          (bytes_of(mid) <= budget ? lo : hi) = mid;
-        }
-        alpha = lo;
-      }
-    }
-    for (size_t i = 0; i < sketched.size(); ++i) caps[i] = cap_of(blk[sketched[i]].B, alpha);
+  for (size_t i = 0; i < sketched.size(); ++i) {
+    const BlockDesc &B = blk[sketched[i]].B;
+    const int C = std::min(B.m, B.n);
+    caps[i] = cap_opt > 0 ? std::min(C, std::max(cap_opt, kPanel)) : C;
   }
   std::vector<SketchBlock> sk;
   for (size_t si = 0; si < sketched.size(); ++si) {
@@ -436,13 +408,38 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   // to a fresh allocation of twice the width, addressed by offsets from
   // `work` like the rest.
   std::vector<double *> grown;
+  const double mem_frac = option("sketch_mem_frac", 0.6);
+  double limited_avail = -1.0;   // device memory seen by the first growth that did not fit
   auto grow = [&](SketchBlock &S, int limit) {
-    const int c2 = std::min(limit, std::max(2 * S.cap, S.cap + kPanel) / kPanel * kPanel);
     const long long wbw = std::max(S.first_w, w_next);
     const long long m = S.m, n = S.n, e = S.ell;
-    const long long sq = align_up(m * c2), sb = align_up(n * c2), sr = align_up((long long)c2 * c2),
-                    st = align_up(c2 * wbw), sc = align_up((long long)c2 * kPanel);
-    const long long total = sq + 2 * sb + sr + st + sc;
+    auto layout = [&](int c2, long long *parts) {
+      parts[0] = align_up(m * c2);
+      parts[1] = align_up(n * c2);
+      parts[2] = align_up((long long)c2 * c2);
+      parts[3] = align_up(c2 * wbw);
+      parts[4] = align_up((long long)c2 * kPanel);
+      return parts[0] + 2 * parts[1] + parts[2] + parts[3] + parts[4];
+    };
+    // twice the width, else smaller steps, whichever fits the memory budget
+    // together with the block's core SVD (about five c2^2 doubles)
+    const double avail = cap_opt > 0 ? 1e300 : device_avail_bytes();
+    int c2 = 0;
+    long long parts[5];
+    for (int cand : {2 * S.cap, S.cap + S.cap / 2, S.cap + 256, S.cap + kPanel}) {
+      const int c = std::min(limit, std::max(cand, S.cap + kPanel) / kPanel * kPanel);
+      if (c <= S.cap) continue;
+      if (8.0 * ((double)layout(c, parts) + 5.0 * (double)c * c) <= mem_frac * avail) {
+        c2 = c;
+        break;
+      }
+    }
+    if (c2 == 0) {
+      if (limited_avail < 0.0) limited_avail = avail;
+      return;
+    }
+    const long long total = layout(c2, parts);
+    const long long sq = parts[0], sb = parts[1], sr = parts[2], st = parts[3];
     double *g = dev_alloc(total, stream);
     grown.push_back(g);
     HB_CUDA(cudaMemsetAsync(g, 0, sizeof(double) * total, stream));
@@ -928,7 +925,9 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     set_last_error(cap_opt > 0
                        ? "a block's rank reached the sketch cap (option sketch_cap)"
                        : "a block's rank reached the sketch width that fits the device memory "
-                         "(option sketch_mem_frac)");
+                         "(option sketch_mem_frac; " +
+                             std::to_string((long long)(limited_avail / 1e9)) +
+                             " GB free or unused in the pool when it could not grow)");
   }
   BuildStats st;
   st.exact_blocks = (int)exact.size();

@@ -69,9 +69,9 @@ const char *hodlr_b200_last_error(void);
  *   sketch_eta (0.01): stopping residual, times tol sigma_0
  *   sketch_cap (0): largest sketch width (a block that needs more ends the
  *       build with SVD_FAILURE); 0 = as wide as memory allows
- *   sketch_mem_frac (0.6): with sketch_cap 0, the share of the free device
- *       memory (including memory the stream-ordered pool holds unused) that
- *       the build's sketches may take
+ *   sketch_mem_frac (0.6): with sketch_cap 0, a block's sketch grows while
+ *       each growth of its scratch (plus its core SVD) fits this share of the
+ *       device memory free or held unused by the stream-ordered pool
  *   sketch_seed (20240607): seed of the Gaussian test matrices
  *   sketch_clean_rel (1e-13): rounding level below which a new panel is zeroed
  *   exact_max (128): blocks with min(m, n) up to this are compressed by an

@@ -191,3 +191,28 @@ def test_failed_device_builds_release_their_trees(lib):
         lib.hodlr_b200_set_option(b"sketch_cap", 0.0)
     # each leaked tree would hold about 5 MB (leaves and factors)
     assert free0 - free1 < 16 * 2 ** 20, (free0, free1)
+
+
+def test_sketch_growth_bounded_by_memory_budget(lib):
+    """A block whose sketch must grow past its starting width (the 3D n = 8192
+    exponential workload's top blocks need about 1500 columns, the start is
+    1024) stops growing when the growth would not fit option sketch_mem_frac
+    of the free device memory: SVD_FAILURE with a message naming the option;
+    with the default budget the same build succeeds and reaches that width."""
+    import torch
+    n, h = 8192, 6
+    pts = W.points_morton(n, 3, 4)
+    d_pts = torch.from_numpy(np.asfortranarray(pts).T.copy().reshape(-1)).cuda()
+    lib.hodlr_b200_set_option(b"sketch_mem_frac", 1e-6)
+    try:
+        with pytest.raises(HodlrError) as e:
+            DeviceTree.build_kernel(d_pts.data_ptr(), n, 3, 2, 0.15, 1e-2, h, 1e-8)
+        assert e.value.code == abi.SVD_FAILURE
+        assert "sketch_mem_frac" in str(e.value)
+    finally:
+        lib.hodlr_b200_set_option(b"sketch_mem_frac", 0.6)
+    t = DeviceTree.build_kernel(d_pts.data_ptr(), n, 3, 2, 0.15, 1e-2, h, 1e-8)
+    st = (C.c_double * 18)()
+    lib.hodlr_b200_build_stats(st, 18)
+    assert st[9] > 1024 and st[4] == 0   # largest sketch, cap hit
+    t.free()
