@@ -376,6 +376,19 @@ bj_pair_kernel(const BjDev *__restrict__ probs, const int2 *__restrict__ slots, 
   rotate_rows(va, vb, Lp, vr0, vr1, S.gp, warp, gq, tq);
 }
 
+// The integer outputs of one problem.
+struct BjIntOut {
+  int *rank, *sweeps;
+  int r, sw;
+};
+
+__global__ void bj_int_out_kernel(const BjIntOut *__restrict__ o, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    *o[i].rank = o[i].r;
+    if (o[i].sweeps) *o[i].sweeps = o[i].sw;
+  }
+}
+
 struct Work {
   int L = 0, Lp = 0, nblk = 0, players = 0, npairs = 0;
   long long x = 0, v = 0;
@@ -432,16 +445,21 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
   // a column pair of length L recomputed by a 64-term sum is orthogonal to
   // about sqrt(L) eps
   const double conv = 8.0 * std::sqrt((double)lmax) * 2.220446049250313e-16;
+  // the column norms of every problem lie in one range of the workspace:
+  // read them in one copy
+  const long long n_lo = noff[0], n_hi = noff[np - 1] + wk[np - 1].Lp;
+  std::vector<double> hn((size_t)(n_hi - n_lo));
+  auto read_norms = [&]() {
+    HB_CUDA(cudaMemcpyAsync(hn.data(), w + n_lo, sizeof(double) * (n_hi - n_lo),
+                            cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+  };
   std::vector<BjDev> hd(np);
   {
-    std::vector<double> h;
+    read_norms();
     for (int p = 0; p < np; ++p) {
-      h.resize(wk[p].Lp);
-      HB_CUDA(cudaMemcpyAsync(h.data(), w + noff[p], sizeof(double) * wk[p].Lp,
-                              cudaMemcpyDeviceToHost, s));
-      HB_CUDA(cudaStreamSynchronize(s));
       double f2 = 0.0;
-      for (double v : h) f2 += v;
+      for (int c = 0; c < wk[p].Lp; ++c) f2 += hn[noff[p] - n_lo + c];
       const Work &W = wk[p];
       // the scalar solver's skip rule for the relative truncation
       const double theta = 1e-3 * tol * std::sqrt(f2) / W.L;
@@ -538,12 +556,11 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
   std::vector<CopyDesc> gather;
   std::vector<std::vector<double>> sig(np);
   std::vector<int> ranks(np), sweeps(np);
+  read_norms();
   for (int p = 0; p < np; ++p) {
     const Work &W = wk[p];
-    std::vector<double> n2(W.Lp);
-    HB_CUDA(cudaMemcpyAsync(n2.data(), w + noff[p], sizeof(double) * W.Lp,
-                            cudaMemcpyDeviceToHost, s));
-    HB_CUDA(cudaStreamSynchronize(s));
+    const std::vector<double> n2(hn.begin() + (noff[p] - n_lo),
+                                 hn.begin() + (noff[p] - n_lo) + W.Lp);
     std::vector<int> perm(W.Lp);
     std::iota(perm.begin(), perm.end(), 0);
     std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return n2[a] > n2[b]; });
@@ -565,15 +582,32 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
   CopyDesc *dg = upload_vec(gather, s);
   copy2d_batched(dg, (int)gather.size(), s);
   cudaFreeAsync(dg, s);
+  // singular values (one upload, scattered by one copy launch), ranks and
+  // sweeps (one launch)
   bool failed = false;
-  for (int p = 0; p < np; ++p) {
-    HB_CUDA(cudaMemcpyAsync(probs[p].sigma, sig[p].data(), sizeof(double) * wk[p].L,
-                            cudaMemcpyHostToDevice, s));
-    HB_CUDA(cudaMemcpyAsync(probs[p].rank, &ranks[p], sizeof(int), cudaMemcpyHostToDevice, s));
-    if (probs[p].sweeps)
-      HB_CUDA(cudaMemcpyAsync(probs[p].sweeps, &sweeps[p], sizeof(int), cudaMemcpyHostToDevice,
-                              s));
-    failed = failed || !wk[p].converged;
+  {
+    std::vector<double> hs;
+    std::vector<long long> so(np);
+    for (int p = 0; p < np; ++p) {
+      so[p] = (long long)hs.size();
+      hs.insert(hs.end(), sig[p].begin(), sig[p].end());
+    }
+    double *ds = upload_vec(hs, s);
+    std::vector<CopyDesc> sc;
+    std::vector<BjIntOut> io;
+    for (int p = 0; p < np; ++p) {
+      sc.push_back(CopyDesc{ds + so[p], wk[p].L, probs[p].sigma, wk[p].L, wk[p].L, 1});
+      io.push_back(BjIntOut{probs[p].rank, probs[p].sweeps, ranks[p], sweeps[p]});
+      failed = failed || !wk[p].converged;
+    }
+    CopyDesc *dsc = upload_vec(sc, s);
+    copy2d_batched(dsc, (int)sc.size(), s);
+    BjIntOut *dio = upload_vec(io, s);
+    bj_int_out_kernel<<<(np + 127) / 128, 128, 0, s>>>(dio, np);
+    HB_LAUNCHED();
+    cudaFreeAsync(dsc, s);
+    cudaFreeAsync(dio, s);
+    cudaFreeAsync(ds, s);
   }
   if (failed) {
     const int st = SVD_FAILURE;

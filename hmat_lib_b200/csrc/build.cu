@@ -85,6 +85,33 @@ double device_avail_bytes() {
   return avail;
 }
 
+// Reads descs[i] (a column of up to `stride` doubles each, dst unused) into
+// row i of `host` (rows of `stride` doubles): one gather launch into
+// stream-ordered staging and one copy back instead of a copy per block.
+// Synchronises with `s`.
+void gather_to_host(std::vector<CopyDesc> descs, int stride, double *host, cudaStream_t s) {
+  if (descs.empty()) return;
+  const int nrow = (int)descs.size();
+  double *stage = dev_alloc((size_t)nrow * stride, s);
+  std::vector<CopyDesc> live;
+  for (int i = 0; i < nrow; ++i) {
+    CopyDesc &d = descs[i];
+    if (d.rows <= 0) continue;
+    d.dst = stage + (long long)i * stride;
+    d.ldd = stride;
+    d.cols = 1;
+    live.push_back(d);
+  }
+  if (!live.empty()) {
+    CopyDesc *dd = upload_vec(live, s);
+    copy2d_batched(dd, (int)live.size(), s);
+    cudaFreeAsync(dd, s);
+  }
+  HB_CUDA(cudaMemcpyAsync(host, stage, sizeof(double) * nrow * stride, cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  dev_free(stage, s);
+}
+
 thread_local BuildStats g_last_stats;
 thread_local std::vector<float> g_last_features;
 
@@ -175,10 +202,11 @@ std::vector<float> block_features(const std::vector<SketchBlock> &sk,
   JacobiProb *d_jp = upload_vec(jp, stream);
   jacobi_svd_batched(d_jp, nsk, prm, d_rank + nsk, F, stream);
   std::vector<double> sig((size_t)nsk * F);
-  for (int i = 0; i < nsk; ++i)
-    HB_CUDA(cudaMemcpyAsync(&sig[(size_t)i * F], w + sg[i], sizeof(double) * F,
-                            cudaMemcpyDeviceToHost, stream));
-  HB_CUDA(cudaStreamSynchronize(stream));
+  {
+    std::vector<CopyDesc> gd;
+    for (int i = 0; i < nsk; ++i) gd.push_back(CopyDesc{w + sg[i], F, nullptr, 0, F, 1});
+    gather_to_host(gd, F, sig.data(), stream);
+  }
   cudaFreeAsync(d_jp, stream);
   cudaFreeAsync(d_rank, stream);
   dev_free(w, stream);
@@ -209,11 +237,11 @@ const std::vector<float> &last_build_features() { return g_last_features; }
 namespace {
 
 // The build.  With sketch_cap 0 every sketched block starts with a modest
-// width cap -- 1024 columns, or twice its predicted one-shot width -- so that
-// a build whose ranks are small never reserves (and maps) scratch for
-// full-width sketches; a block that reaches that cap while its
-// memory-bounded cap is larger moves its sketch into scratch of twice the
-// width (up to the memory-bounded cap) and carries on.
+// width cap -- 256 columns (option sketch_start), or twice its predicted
+// one-shot width -- so that a build whose ranks are small never reserves (and
+// maps) scratch for wide sketches; a block that fills it moves its sketch
+// into scratch of twice the width while the device memory allows (grow())
+// and carries on.
 std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     const std::vector<BuildInput> &in, double tol, cudaStream_t stream, int *svd_status,
     BuildStats *stats, const KernelSpec *gen, std::chrono::steady_clock::time_point t0) {
@@ -367,13 +395,15 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
       }
     }
   }
-  // starting caps: 1024 columns or twice the one-shot width (grown on demand)
+  // starting caps: option sketch_start (256) columns or twice the one-shot
+  // width, grown on demand
+  const int start_cap = std::max(2 * kPanel, (int)option("sketch_start", 256) / kPanel * kPanel);
   std::vector<int> memcap(sk.size());
   for (size_t i = 0; i < sk.size(); ++i) {
     SketchBlock &S = sk[i];
     memcap[i] = S.cap;
     if (cap_opt <= 0) {
-      const int want = std::max(1024, (2 * S.first_w + kPanel - 1) / kPanel * kPanel);
+      const int want = std::max(start_cap, (2 * S.first_w + kPanel - 1) / kPanel * kPanel);
       S.cap = std::min(S.cap, want);
     }
   }
@@ -483,6 +513,8 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   cudaEvent_t ev[5];
   for (auto &e : ev) HB_CUDA(cudaEventCreate(&e));
   HB_CUDA(cudaEventRecord(ev[0], stream));
+  const double ms_setup =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 
   // ---- exact path ----------------------------------------------------------------
   std::vector<JacobiProb> eprobs;
@@ -713,15 +745,28 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
       column_norms2(nd, stream);
     }
     // 8. read back and decide
+    // per active block: its row norms of B (wb values, row 2a) and its last
+    // panel's residual column norms (last_pw values, row 2a + 1), gathered and
+    // read back in one copy
     std::vector<double> bn(act.size() * w_max, 0.0), rcols(act.size() * kPanel, 0.0);
-    for (size_t a = 0; a < act.size(); ++a) {
-      const SketchBlock &S = sk[act[a]];
-      HB_CUDA(cudaMemcpyAsync(&bn[a * w_max], work + S.t, sizeof(double) * wb[act[a]],
-                              cudaMemcpyDeviceToHost, stream));
-      HB_CUDA(cudaMemcpyAsync(&rcols[a * kPanel], work + S.rn + kPanel * kPanel,
-                              sizeof(double) * S.last_pw, cudaMemcpyDeviceToHost, stream));
+    {
+      const int stride = std::max(w_max, kPanel);
+      std::vector<CopyDesc> gd;
+      for (size_t a = 0; a < act.size(); ++a) {
+        const SketchBlock &S = sk[act[a]];
+        gd.push_back(CopyDesc{work + S.t, (long long)std::max(wb[act[a]], 1), nullptr, 0,
+                              wb[act[a]], 1});
+        gd.push_back(CopyDesc{work + S.rn + kPanel * kPanel, kPanel, nullptr, 0, S.last_pw, 1});
+      }
+      std::vector<double> h(gd.size() * (size_t)stride, 0.0);
+      gather_to_host(gd, stride, h.data(), stream);
+      for (size_t a = 0; a < act.size(); ++a) {
+        std::copy(h.begin() + (2 * a) * stride, h.begin() + (2 * a) * stride + wb[act[a]],
+                  bn.begin() + a * w_max);
+        std::copy(h.begin() + (2 * a + 1) * stride, h.begin() + (2 * a + 1) * stride + kPanel,
+                  rcols.begin() + a * kPanel);
+      }
     }
-    HB_CUDA(cudaStreamSynchronize(stream));
     for (size_t a = 0; a < act.size(); ++a) {
       SketchBlock &S = sk[act[a]];
       double f2 = 0.0;
@@ -967,6 +1012,8 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   st.ms_core_svd = stage_ms[2];
   st.ms_finish = stage_ms[3];
   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  st.ms_host_setup = ms_setup;
+  st.ms_host_total = 1e3 * st.seconds;
   g_last_stats = st;
   if (stats) *stats = st;
   return dts;

@@ -26,6 +26,8 @@ struct BuildStats {
   double ms_features = 0.0;    // rank-model features and prediction (host clock)
   double gemm_flops = 0.0;     // FP64 GEMM work of the build (2 M N K summed)
   double input_elems = 0.0;    // entries of the input matrices (n^2 per tree)
+  double ms_host_setup = 0.0;  // host clock from the call to the first stage event
+  double ms_host_total = 0.0;  // host clock from the call to the return
 };
 
 // Statistics of the most recent build on the calling thread.

@@ -67,6 +67,8 @@ const char *hodlr_b200_last_error(void);
  *   sketch_first (64), sketch_step (64): first and later widths of the
  *       adaptive range finder's rounds
  *   sketch_eta (0.01): stopping residual, times tol sigma_0
+ *   sketch_start (256): starting sketch scratch width of a block (or twice its
+ *       one-shot width); grown 2x in place when it fills
  *   sketch_cap (0): largest sketch width (a block that needs more ends the
  *       build with SVD_FAILURE); 0 = as wide as memory allows
  *   sketch_mem_frac (0.6): with sketch_cap 0, a block's sketch grows while
@@ -210,8 +212,9 @@ int hodlr_b200_phase_times(double *out, int capacity);
  * then the device milliseconds of the stages: small-block SVDs, sketch
  * rounds, SVDs of the sketched cores, finishing; one-shot sketches that fell
  * back to adaptive growth; milliseconds of the rank-model features and
- * prediction; FP64 GEMM work (flops, 2 M N K summed) and input entries.
- * Returns the number of values. */
+ * prediction; FP64 GEMM work (flops, 2 M N K summed) and input entries;
+ * host milliseconds from the call to the first stage.  Returns the number of
+ * values. */
 int hodlr_b200_build_stats(double *out, int capacity);
 /* y = H x on device buffers, allocating nothing (no counterpart in hmat_lib).
  * For callers that cannot allocate device memory while they run: an

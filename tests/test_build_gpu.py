@@ -196,7 +196,7 @@ def test_failed_device_builds_release_their_trees(lib):
 def test_sketch_growth_bounded_by_memory_budget(lib):
     """A block whose sketch must grow past its starting width (the 3D n = 8192
     exponential workload's top blocks need about 1500 columns, the start is
-    1024) stops growing when the growth would not fit option sketch_mem_frac
+    256) stops growing when the growth would not fit option sketch_mem_frac
     of the free device memory: SVD_FAILURE with a message naming the option;
     with the default budget the same build succeeds and reaches that width."""
     import torch
