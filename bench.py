@@ -187,14 +187,14 @@ def run_cpu_baseline(n: int, k: int, steps: int = 3, warmup: int = 1, extra=()):
 
 def build_stats(lib):
     """Stage times and counters of the calling thread's latest build."""
-    st = (C.c_double * 19)()
-    lib.hodlr_b200_build_stats(st, 19)
+    st = (C.c_double * 20)()
+    lib.hodlr_b200_build_stats(st, 20)
     return {"library_seconds": st[3], "exact_blocks": int(st[0]),
             "sketched_blocks": int(st[1]), "sketch_rounds": int(st[2]),
             "largest_sketch": int(st[9]), "ms_small_svd": st[10], "ms_rounds": st[11],
             "ms_core_svd": st[12], "ms_finish": st[13], "learned_fallbacks": int(st[14]),
             "ms_features": st[15], "gemm_flops": st[16], "input_elems": st[17],
-            "ms_host_setup": st[18]}
+            "ms_host_setup": st[18], "ms_host_plans": st[19]}
 
 
 def build_roofline(stats, seconds, storage, peak_tflops, peak_gbs, matrix_free=False):
@@ -573,7 +573,7 @@ def uneven_batch_bench(count, steps, warmup, lib, torch, dev, stream, pg=None, r
             batched_s += time.perf_counter() - t0
             bst = build_stats(lib)
             for key in ("ms_small_svd", "ms_rounds", "ms_core_svd", "ms_finish", "ms_host_setup",
-                        "library_seconds"):
+                        "ms_host_plans", "library_seconds"):
                 batched_stages[key] = batched_stages.get(key, 0.0) + bst[key]
             batched_stages["sketch_rounds"] = max(batched_stages.get("sketch_rounds", 0),
                                                   bst["sketch_rounds"])

@@ -857,7 +857,7 @@ int hodlr_b200_build_stats(double *out, int capacity) {
                       st.ms_core_svd,              st.ms_finish,
                       (double)st.learned_fallbacks, st.ms_features,
                       st.gemm_flops,               st.input_elems,
-                      st.ms_host_setup};
+                      st.ms_host_setup,            st.ms_host_plans};
   const int n = (int)(sizeof(v) / sizeof(v[0]));
   for (int i = 0; i < n && i < capacity && out; ++i) out[i] = v[i];
   return n;

@@ -237,8 +237,8 @@ const std::vector<float> &last_build_features() { return g_last_features; }
 namespace {
 
 // The build.  With sketch_cap 0 every sketched block starts with a modest
-// width cap -- 256 columns (option sketch_start), or twice its predicted
-// one-shot width -- so that a build whose ranks are small never reserves (and
+// width cap -- 256 columns (option sketch_start) or an eighth of its width, or
+// twice its predicted one-shot width -- so that a build whose ranks are small never reserves (and
 // maps) scratch for wide sketches; a block that fills it moves its sketch
 // into scratch of twice the width while the device memory allows (grow())
 // and carries on.
@@ -395,15 +395,19 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
       }
     }
   }
-  // starting caps: option sketch_start (256) columns or twice the one-shot
-  // width, grown on demand
+  // starting caps: option sketch_start (256) columns, an eighth of the width
+  // if that is more, or twice the one-shot width; grown on demand
   const int start_cap = std::max(2 * kPanel, (int)option("sketch_start", 256) / kPanel * kPanel);
   std::vector<int> memcap(sk.size());
   for (size_t i = 0; i < sk.size(); ++i) {
     SketchBlock &S = sk[i];
     memcap[i] = S.cap;
     if (cap_opt <= 0) {
-      const int want = std::max(start_cap, (2 * S.first_w + kPanel - 1) / kPanel * kPanel);
+      // blocks wider than 8 start_cap columns start at an eighth of their
+      // width (a wide block's rank can reach thousands: fewer growths, each a
+      // fresh allocation of several GB)
+      const int base = std::max(start_cap, std::min(S.m, S.n) / 8 / kPanel * kPanel);
+      const int want = std::max(base, (2 * S.first_w + kPanel - 1) / kPanel * kPanel);
       S.cap = std::min(S.cap, want);
     }
   }
@@ -508,6 +512,10 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   prm.trunc = Truncation::Relative;
   prm.scale_u = 1;
   prm.max_sweeps = (int)option("jacobi_max_sweeps", 60);
+  // a pair coupled at rounding level of the block's own norm counts as
+  // orthogonal: it moves no singular value by more than eps ||A||, far below
+  // the truncation threshold tol sigma_0
+  prm.norm_stop = option("jacobi_norm_stop", 1.0) != 0.0 ? 1 : 0;
 
   // stage events: start, exact done, rounds done, core SVDs done, end
   cudaEvent_t ev[5];
@@ -1014,6 +1022,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   st.ms_host_setup = ms_setup;
   st.ms_host_total = 1e3 * st.seconds;
+  st.ms_host_plans = plan_host_ms();
   g_last_stats = st;
   if (stats) *stats = st;
   return dts;
@@ -1027,6 +1036,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_batch(const std::vector<BuildInpu
                                                      const KernelSpec *gen) {
   const auto t0 = std::chrono::steady_clock::now();
   gemm_flops_counter() = 0.0;
+  plan_host_ms() = 0.0;
   return build_attempt(in, tol, stream, svd_status, stats, gen, t0);
 }
 

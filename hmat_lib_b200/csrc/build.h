@@ -28,6 +28,7 @@ struct BuildStats {
   double input_elems = 0.0;    // entries of the input matrices (n^2 per tree)
   double ms_host_setup = 0.0;  // host clock from the call to the first stage event
   double ms_host_total = 0.0;  // host clock from the call to the return
+  double ms_host_plans = 0.0;  // host clock spent making GEMM and TSQR plans
 };
 
 // Statistics of the most recent build on the calling thread.

@@ -8,6 +8,7 @@
 // memory as double2.  FP64 has no tcgen05 path; this is the FP64 roofline
 // kernel (B200: 64 DFMA / clock / SM).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -20,6 +21,11 @@ int gemm_f64_engine() { return (int)option("gemm_f64_engine", 2); }
 double &gemm_flops_counter() {
   static thread_local double flops = 0.0;
   return flops;
+}
+
+double &plan_host_ms() {
+  static thread_local double ms = 0.0;
+  return ms;
 }
 
 namespace {
@@ -554,6 +560,14 @@ GemmPlan::~GemmPlan() {
 
 void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool allow_split,
                      cudaStream_t stream, bool transient) {
+  const auto t_start = std::chrono::steady_clock::now();
+  struct Clock {
+    std::chrono::steady_clock::time_point t;
+    ~Clock() {
+      plan_host_ms() +=
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+    }
+  } clock{t_start};
   const int BM = tile_rows(shape);
   const int BN = tile_cols(shape);
   plan.shape = shape;

@@ -121,6 +121,9 @@ void gemm_plan_run(const GemmPlan &plan, const GemmBases &bases, cudaStream_t st
 // FP64 multiply-add work (2 M N K per problem) of every GEMM plan built on
 // the calling thread since the counter was last reset (build statistics).
 double &gemm_flops_counter();
+// Host milliseconds spent making GEMM and TSQR plans on this thread (reset by
+// the caller).
+double &plan_host_ms();
 
 // Which kernel runs the FP64 products (option gemm_f64_engine): 1 the FP64
 // tensor-core (DMMA) kernel, 0 the DFMA kernel.

@@ -149,6 +149,7 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
     theta = 1e-3 * prm.tol / sqrt((double)C);
   theta = fmax(theta, P.skip_abs);
   const double skip2 = theta * theta;
+  const double cscale = P.conv_scale > 0.0 ? P.conv_scale : (prm.norm_stop ? sqrt(f2) : 0.0);
 
   // a computed dot product of length R carries ~sqrt(R) eps relative noise:
   // below that no rotation can make progress
@@ -200,8 +201,7 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
         // coupling at rounding level of the problem's own scale (a block of a
         // larger matrix, whose columns were recomputed by a GEMM) counts as
         // converged: it moves no singular value by more than that level
-        if (P.conv_scale > 0.0)
-          rel = fmin(rel, fabs(ga) / (P.conv_scale * fmax(sqrt(al), sqrt(be))));
+        if (cscale > 0.0) rel = fmin(rel, fabs(ga) / (cscale * fmax(sqrt(al), sqrt(be))));
         off = fmax(off, rel);
         if (rel <= conv) continue;
         const double zeta = (be - al) / (2.0 * ga);

@@ -46,6 +46,9 @@ struct JacobiParams {
   int scale_u = 1;          // write U * Sigma (hmat_lib stores scaled U)
   int max_sweeps = 60;      // bounded: exceeding it sets the status word
   double conv_tol = 1e-15;  // |g_p . g_q| <= conv_tol ||g_p|| ||g_q||
+  // problems without their own conv_scale take ||A||_F: a pair also counts as
+  // orthogonal when |g_p . g_q| <= conv_tol ||A||_F max(||g_p||, ||g_q||)
+  int norm_stop = 0;
 };
 
 // Workspace doubles needed by problem (m, n): G + W.

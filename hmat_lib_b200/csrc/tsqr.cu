@@ -7,7 +7,9 @@
 // 126) and provides the orthonormal bases of the randomized range finder
 // that stands in for dgesdd on large blocks (src/constructors.c:323).
 #include <algorithm>
+#include <chrono>
 
+#include "gemm_f64.h"
 #include "tsqr.h"
 
 namespace hb {
@@ -277,6 +279,13 @@ void TsqrPlanDeleter::operator()(TsqrPlan *p) const { delete p; }
 
 std::unique_ptr<TsqrPlan, TsqrPlanDeleter> tsqr_plan(const std::vector<TsqrProb> &probs,
                                                      cudaStream_t s) {
+  struct Clock {
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    ~Clock() {
+      plan_host_ms() +=
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+    }
+  } clock;
   std::unique_ptr<TsqrPlan, TsqrPlanDeleter> plan(new TsqrPlan);
   plan->stream = s;
   if (probs.empty()) return plan;

@@ -67,8 +67,9 @@ const char *hodlr_b200_last_error(void);
  *   sketch_first (64), sketch_step (64): first and later widths of the
  *       adaptive range finder's rounds
  *   sketch_eta (0.01): stopping residual, times tol sigma_0
- *   sketch_start (256): starting sketch scratch width of a block (or twice its
- *       one-shot width); grown 2x in place when it fills
+ *   sketch_start (256): starting sketch scratch width of a block (or an eighth
+ *       of its width, or twice its one-shot width, if more); grown 2x in place
+ *       when it fills
  *   sketch_cap (0): largest sketch width (a block that needs more ends the
  *       build with SVD_FAILURE); 0 = as wide as memory allows
  *   sketch_mem_frac (0.6): with sketch_cap 0, a block's sketch grows while
@@ -79,6 +80,9 @@ const char *hodlr_b200_last_error(void);
  *   exact_max (128): blocks with min(m, n) up to this are compressed by an
  *       exact Jacobi SVD
  *   jacobi_max_sweeps (60): Jacobi sweep bound (SVD_FAILURE past it)
+ *   jacobi_norm_stop (1): in the build's Jacobi SVDs a column pair also counts
+ *       as orthogonal when its product is at rounding level of eps ||A||_F
+ *       times the larger column norm (0: the scaled test alone)
  *   jacobi_cluster_min_c (192): problems this wide or wider use a cluster of
  *       8 CTAs
  *   jacobi_block_min_c (128): sketch cores this wide or wider are solved by
@@ -213,8 +217,8 @@ int hodlr_b200_phase_times(double *out, int capacity);
  * rounds, SVDs of the sketched cores, finishing; one-shot sketches that fell
  * back to adaptive growth; milliseconds of the rank-model features and
  * prediction; FP64 GEMM work (flops, 2 M N K summed) and input entries;
- * host milliseconds from the call to the first stage.  Returns the number of
- * values. */
+ * host milliseconds from the call to the first stage and spent making GEMM
+ * and TSQR plans.  Returns the number of values. */
 int hodlr_b200_build_stats(double *out, int capacity);
 /* y = H x on device buffers, allocating nothing (no counterpart in hmat_lib).
  * For callers that cannot allocate device memory while they run: an
