@@ -512,10 +512,11 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   prm.trunc = Truncation::Relative;
   prm.scale_u = 1;
   prm.max_sweeps = (int)option("jacobi_max_sweeps", 60);
-  // a pair coupled at rounding level of the block's own norm counts as
-  // orthogonal: it moves no singular value by more than eps ||A||, far below
-  // the truncation threshold tol sigma_0
-  prm.norm_stop = option("jacobi_norm_stop", 1.0) != 0.0 ? 1 : 0;
+  // option: a pair coupled at rounding level of the block's own norm counts as
+  // orthogonal (moves no singular value by more than eps ||A||), fewer sweeps;
+  // off by default: the normalised columns of the rotated side (hmat_lib's
+  // orthonormal U or V) then keep couplings of up to eps ||A|| / sigma
+  prm.norm_stop = option("jacobi_norm_stop", 0.0) != 0.0 ? 1 : 0;
 
   // stage events: start, exact done, rounds done, core SVDs done, end
   cudaEvent_t ev[5];

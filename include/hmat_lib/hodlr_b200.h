@@ -80,9 +80,11 @@ const char *hodlr_b200_last_error(void);
  *   exact_max (128): blocks with min(m, n) up to this are compressed by an
  *       exact Jacobi SVD
  *   jacobi_max_sweeps (60): Jacobi sweep bound (SVD_FAILURE past it)
- *   jacobi_norm_stop (1): in the build's Jacobi SVDs a column pair also counts
- *       as orthogonal when its product is at rounding level of eps ||A||_F
- *       times the larger column norm (0: the scaled test alone)
+ *   jacobi_norm_stop (0): 1 = in the build's one-CTA / cluster Jacobi SVDs a
+ *       column pair also counts as orthogonal when its product is at rounding
+ *       level of eps ||A||_F times the larger column norm (fewer sweeps; the
+ *       singular vectors of small singular values are then orthogonal only to
+ *       about eps ||A|| / sigma)
  *   jacobi_cluster_min_c (192): problems this wide or wider use a cluster of
  *       8 CTAs
  *   jacobi_block_min_c (128): sketch cores this wide or wider are solved by
