@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 
 #include "gemm_f64.h"
 
@@ -584,13 +585,12 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
     work += (double)mn * (double)std::max<long long>(ktot[p], 1);
   }
   const long long target = 4LL * num_sms();
-  std::vector<GemmTile> tiles;
-  tiles.reserve(base_tiles);
+  // per problem: its K split and the K length of its tiles
   plan.any_split = false;
+  std::vector<long long> chunk_of(probs.size(), 0);
   for (size_t p = 0; p < probs.size(); ++p) {
     GemmProb &P = probs[p];
     if (P.M <= 0 || P.N <= 0) continue;
-    const int mt = (P.M + BM - 1) / BM, nt = (P.N + BN - 1) / BN;
     // Split K so that no tile carries much more than an even share of the
     // batch's work (the longest tile bounds the launch), and to fill the GPU.
     long long split = 1;
@@ -606,23 +606,35 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
     split = std::max<long long>(1, (ktot[p] + chunk - 1) / chunk);
     P.split = (int)split;
     if (split > 1) plan.any_split = true;
+    chunk_of[p] = split == 1 ? ktot[p] : chunk;
+  }
+  // tiles of the problems with the longest K ranges first, for load balance
+  // (ordering the problems, not the tiles: a problem's tiles share their K
+  // length but for a shorter last split)
+  std::vector<int> order(probs.size());
+  for (size_t p = 0; p < probs.size(); ++p) order[p] = (int)p;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return chunk_of[a] > chunk_of[b]; });
+  std::vector<GemmTile> tiles;
+  tiles.reserve(base_tiles);
+  for (int p : order) {
+    const GemmProb &P = probs[p];
+    if (P.M <= 0 || P.N <= 0) continue;
+    const int mt = (P.M + BM - 1) / BM, nt = (P.N + BN - 1) / BN;
+    const long long chunk = chunk_of[p];
     for (int mi = 0; mi < mt; ++mi)
       for (int ni = 0; ni < nt; ++ni)
-        for (long long si = 0; si < split; ++si) {
+        for (long long si = 0; si < P.split; ++si) {
           GemmTile t;
-          t.prob = (int)p;
+          t.prob = p;
           t.m0 = mi * BM;
           t.n0 = ni * BN;
           t.k0 = (int)(si * chunk);
           t.k1 = (int)std::min<long long>(ktot[p], (si + 1) * chunk);
-          if (split == 1) t.k1 = (int)ktot[p];
+          if (P.split == 1) t.k1 = (int)ktot[p];
           tiles.push_back(t);
         }
   }
-  // longest K ranges first for load balance
-  std::stable_sort(tiles.begin(), tiles.end(), [](const GemmTile &a, const GemmTile &b) {
-    return (a.k1 - a.k0) > (b.k1 - b.k0);
-  });
   plan.ntiles = (int)tiles.size();
   plan.nprobs = (int)probs.size();
   const size_t bs = batch.segs.size() * sizeof(GemmSeg);
@@ -646,13 +658,13 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
   plan.segs = (GemmSeg *)base;
   plan.probs = (GemmProb *)(base + align_up(bs, 256));
   plan.tiles = (GemmTile *)(base + align_up(bs, 256) + align_up(bp, 256));
-  std::vector<char> host(total, 0);
-  if (bs) std::memcpy(host.data(), batch.segs.data(), bs);
-  if (bp) std::memcpy(host.data() + align_up(bs, 256), probs.data(), bp);
-  if (bt) std::memcpy(host.data() + align_up(bs, 256) + align_up(bp, 256), tiles.data(), bt);
+  std::unique_ptr<char[]> host(new char[total]);   // padding bytes are never read
+  if (bs) std::memcpy(host.get(), batch.segs.data(), bs);
+  if (bp) std::memcpy(host.get() + align_up(bs, 256), probs.data(), bp);
+  if (bt) std::memcpy(host.get() + align_up(bs, 256) + align_up(bp, 256), tiles.data(), bt);
   // pageable source: staged by the driver before the call returns, so the
   // host buffer may go away at once
-  HB_CUDA(cudaMemcpyAsync(plan.dev, host.data(), total, cudaMemcpyHostToDevice, stream));
+  HB_CUDA(cudaMemcpyAsync(plan.dev, host.get(), total, cudaMemcpyHostToDevice, stream));
   if (!transient) HB_CUDA(cudaStreamSynchronize(stream));
 }
 

@@ -205,34 +205,6 @@ T *upload(const std::vector<T> &v, cudaStream_t s) {
   return d;
 }
 
-void launch_qr(const std::vector<QrChunk> &chunks, cudaStream_t s) {
-  if (chunks.empty()) return;
-  static bool configured = false;
-  if (!configured) {
-    HB_CUDA(cudaFuncSetAttribute(qr_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kQrSmem));
-    configured = true;
-  }
-  QrChunk *d = upload(chunks, s);
-  for (size_t off = 0; off < chunks.size(); off += 65535) {
-    const int cnt = (int)std::min<size_t>(65535, chunks.size() - off);
-    qr_chunk_kernel<<<cnt, kQT, kQrSmem, s>>>(d + off);
-    HB_LAUNCHED();
-  }
-  cudaFreeAsync(d, s);
-}
-
-void launch_mul(const std::vector<MulChunk> &chunks, cudaStream_t s) {
-  if (chunks.empty()) return;
-  MulChunk *d = upload(chunks, s);
-  for (size_t off = 0; off < chunks.size(); off += 65535) {
-    const int cnt = (int)std::min<size_t>(65535, chunks.size() - off);
-    mul_chunk_kernel<<<cnt, kQT, 0, s>>>(d + off);
-    HB_LAUNCHED();
-  }
-  cudaFreeAsync(d, s);
-}
-
 __global__ void panel_clean_kernel(const CleanDesc *__restrict__ descs, double rel) {
   const CleanDesc D = descs[blockIdx.y];
   double scale2 = 0.0;
@@ -297,40 +269,52 @@ std::unique_ptr<TsqrPlan, TsqrPlanDeleter> tsqr_plan(const std::vector<TsqrProb>
     int rows;
     int nchunks;
   };
-  std::vector<std::vector<Level>> levels(probs.size());
+  // levels of problem p: lev[lo[p] .. lo[p + 1]) (flat, no per-problem
+  // allocations: a round of the build makes plans for thousands of panels)
+  constexpr int kMaxLevels = 16;
+  std::vector<Level> lev;
+  std::vector<int> lo(probs.size() + 1, 0);
+  lev.reserve(probs.size() * 3);
   long long scratch = 0;
-  std::vector<std::vector<long long>> stack_off(probs.size());
+  std::vector<long long> stack_off;   // per level >= 1, same indexing as lev
+  stack_off.reserve(probs.size() * 3);
   for (size_t p = 0; p < probs.size(); ++p) {
     const TsqrProb &P = probs[p];
     HB_REQUIRE(P.w >= 1 && P.w <= kPanel, INPUT_ERROR, "TSQR panel wider than 32 columns");
+    lo[p] = (int)lev.size();
     int rows = P.m;
-    while (true) {
+    long long off = -1;   // stacked-R scratch of this level (-1: the panel itself)
+    for (int l = 0; l < kMaxLevels; ++l) {
       const int nch = std::max(1, (rows + kChunk - 1) / kChunk);
-      levels[p].push_back(Level{nullptr, 0, rows, nch});
+      lev.push_back(Level{nullptr, 0, rows, nch});
+      stack_off.push_back(off);
       if (nch == 1) break;
       rows = nch * P.w;
-      stack_off[p].push_back(scratch);
+      off = scratch;
       scratch += align_up((long long)rows * P.w);
     }
   }
+  lo[probs.size()] = (int)lev.size();
   if (scratch) HB_CUDA(cudaMallocAsync((void **)&plan->buf, scratch * sizeof(double), s));
   int max_levels = 0;
   for (size_t p = 0; p < probs.size(); ++p) {
-    auto &L = levels[p];
+    Level *L = lev.data() + lo[p];
+    const int nl = lo[p + 1] - lo[p];
     L[0].A = probs[p].Y;
     L[0].lda = probs[p].ldy;
-    for (size_t l = 1; l < L.size(); ++l) {
-      L[l].A = plan->buf + stack_off[p][l - 1];
+    for (int l = 1; l < nl; ++l) {
+      L[l].A = plan->buf + stack_off[lo[p] + l];
       L[l].lda = L[l].rows;
     }
-    max_levels = std::max(max_levels, (int)L.size());
+    max_levels = std::max(max_levels, nl);
   }
   // up-sweep
   for (int l = 0; l < max_levels; ++l) {
     std::vector<QrChunk> chunks;
     for (size_t p = 0; p < probs.size(); ++p) {
-      auto &L = levels[p];
-      if (l >= (int)L.size()) continue;
+      const Level *L = lev.data() + lo[p];
+      const int nl = lo[p + 1] - lo[p];
+      if (l >= nl) continue;
       const int w = probs[p].w;
       for (int c = 0; c < L[l].nchunks; ++c) {
         QrChunk q;
@@ -338,7 +322,7 @@ std::unique_ptr<TsqrPlan, TsqrPlanDeleter> tsqr_plan(const std::vector<TsqrProb>
         q.lda = L[l].lda;
         q.rows = std::min(kChunk, L[l].rows - c * kChunk);
         q.w = w;
-        if (l + 1 < (int)L.size()) {
+        if (l + 1 < nl) {
           q.R = L[l + 1].A + (long long)c * w;
           q.ldr = L[l + 1].lda;
         } else {
@@ -355,8 +339,9 @@ std::unique_ptr<TsqrPlan, TsqrPlanDeleter> tsqr_plan(const std::vector<TsqrProb>
   for (int l = max_levels - 2; l >= 0; --l) {
     std::vector<MulChunk> chunks;
     for (size_t p = 0; p < probs.size(); ++p) {
-      auto &L = levels[p];
-      if (l + 1 >= (int)L.size()) continue;
+      const Level *L = lev.data() + lo[p];
+      const int nl = lo[p + 1] - lo[p];
+      if (l + 1 >= nl) continue;
       const int w = probs[p].w;
       for (int c = 0; c < L[l].nchunks; ++c) {
         MulChunk mc;
