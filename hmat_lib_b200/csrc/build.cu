@@ -42,7 +42,7 @@ T *upload_vec(const std::vector<T> &v, cudaStream_t s) {
   T *d = nullptr;
   HB_CUDA(cudaMallocAsync((void **)&d, sizeof(T) * std::max<size_t>(v.size(), 1), s));
   if (!v.empty())
-    HB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+    h2d_async(d, v.data(), sizeof(T) * v.size(), s);
   return d;
 }
 

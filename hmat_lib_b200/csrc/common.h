@@ -19,6 +19,16 @@ struct Error {
   std::string msg;
 };
 
+// Host -> device copy of `bytes` from pageable memory that returns without
+// waiting for `stream`: the bytes go through a pinned staging ring of the
+// calling thread (64 MiB per device, slots recycled once their copy has
+// completed); `src` may be reused at once.  A copy from pageable memory would
+// make the host wait until the stream reaches it, so a build that uploads
+// launch descriptors between launches would run host and GPU in turn.
+// Copies larger than half the ring, or into a capturing stream, are plain
+// cudaMemcpyAsync calls.
+void h2d_async(void *dst, const void *src, size_t bytes, cudaStream_t stream);
+
 void set_last_error(const std::string &msg);
 // Records a message that is a string literal, without allocating.
 void set_last_error_static(const char *msg);

@@ -1,5 +1,7 @@
 // Device tree arena, upload / download and the host-tree registry.
 #include <atomic>
+#include <deque>
+#include <vector>
 #include <cstring>
 #include <unordered_map>
 
@@ -84,6 +86,86 @@ double *dev_alloc(size_t elems, cudaStream_t stream) {
 
 void dev_free(void *p, cudaStream_t stream) {
   if (p) cudaFreeAsync(p, stream);
+}
+
+namespace {
+
+struct PinnedRing {
+  char *base = nullptr;
+  size_t cap = 0, head = 0;
+  bool tried = false;
+  struct Span {
+    size_t lo, hi;
+    cudaEvent_t ev;
+  };
+  std::deque<Span> live;
+  std::vector<cudaEvent_t> spare;
+  ~PinnedRing() {
+    for (Span &sp : live) cudaEventSynchronize(sp.ev);
+    for (Span &sp : live) cudaEventDestroy(sp.ev);
+    for (cudaEvent_t e : spare) cudaEventDestroy(e);
+    if (base) cudaFreeHost(base);
+    (void)cudaGetLastError();
+  }
+};
+
+constexpr size_t kRingBytes = size_t(64) << 20;
+
+}  // namespace
+
+void h2d_async(void *dst, const void *src, size_t bytes, cudaStream_t stream) {
+  if (bytes == 0) return;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  HB_CUDA(cudaStreamIsCapturing(stream, &cap));
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  thread_local std::unordered_map<int, PinnedRing> rings;
+  PinnedRing &R = rings[dev];
+  if (!R.tried) {
+    R.tried = true;
+    if (cudaMallocHost((void **)&R.base, kRingBytes) == cudaSuccess) {
+      R.cap = kRingBytes;
+    } else {
+      (void)cudaGetLastError();
+      R.base = nullptr;
+    }
+  }
+  const size_t need = (bytes + 255) / 256 * 256;
+  if (cap != cudaStreamCaptureStatusNone || !R.base || need > R.cap / 2) {
+    HB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+    return;
+  }
+  // retire finished copies, oldest first
+  while (!R.live.empty() && cudaEventQuery(R.live.front().ev) == cudaSuccess) {
+    R.spare.push_back(R.live.front().ev);
+    R.live.pop_front();
+  }
+  (void)cudaGetLastError();   // cudaErrorNotReady from the last query
+  size_t lo = R.head;
+  if (lo + need > R.cap) lo = 0;
+  const size_t hi = lo + need;
+  // wait for every copy still reading the slot
+  for (auto it = R.live.begin(); it != R.live.end();) {
+    if (it->lo < hi && lo < it->hi) {
+      HB_CUDA(cudaEventSynchronize(it->ev));
+      R.spare.push_back(it->ev);
+      it = R.live.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  std::memcpy(R.base + lo, src, bytes);
+  HB_CUDA(cudaMemcpyAsync(dst, R.base + lo, bytes, cudaMemcpyHostToDevice, stream));
+  cudaEvent_t ev;
+  if (!R.spare.empty()) {
+    ev = R.spare.back();
+    R.spare.pop_back();
+  } else {
+    HB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  HB_CUDA(cudaEventRecord(ev, stream));
+  R.live.push_back(PinnedRing::Span{lo, hi, ev});
+  R.head = hi;
 }
 
 std::unique_ptr<DeviceTree> dtree_create(const Geometry &g_in, cudaStream_t stream) {

@@ -84,6 +84,7 @@ void keep_pool_memory();
 double *dev_alloc(size_t elems, cudaStream_t stream);
 void dev_free(void *p, cudaStream_t stream);
 
+
 }  // namespace hb
 
 // The opaque handle of include/hmat_lib/hodlr_b200.h.

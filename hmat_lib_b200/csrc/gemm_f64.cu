@@ -662,9 +662,9 @@ void gemm_plan_build(GemmPlan &plan, GemmBatch &batch, TileShape shape, bool all
   if (bs) std::memcpy(host.get(), batch.segs.data(), bs);
   if (bp) std::memcpy(host.get() + align_up(bs, 256), probs.data(), bp);
   if (bt) std::memcpy(host.get() + align_up(bs, 256) + align_up(bp, 256), tiles.data(), bt);
-  // pageable source: staged by the driver before the call returns, so the
-  // host buffer may go away at once
-  HB_CUDA(cudaMemcpyAsync(plan.dev, host.get(), total, cudaMemcpyHostToDevice, stream));
+  // staged through the pinned ring: the host buffer may go away at once, and
+  // the host does not wait for the stream
+  h2d_async(plan.dev, host.get(), total, stream);
   if (!transient) HB_CUDA(cudaStreamSynchronize(stream));
 }
 

@@ -17,7 +17,7 @@ T *upload(const std::vector<T> &v, cudaStream_t s, std::vector<void *> &keep) {
   HB_CUDA(cudaMalloc((void **)&d, sizeof(T) * std::max<size_t>(v.size(), 1)));
   keep.push_back(d);
   if (!v.empty())
-    HB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+    h2d_async(d, v.data(), sizeof(T) * v.size(), s);
   return d;
 }
 

@@ -201,7 +201,7 @@ template <class T>
 T *upload(const std::vector<T> &v, cudaStream_t s) {
   T *d = nullptr;
   HB_CUDA(cudaMallocAsync((void **)&d, sizeof(T) * std::max<size_t>(v.size(), 1), s));
-  HB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  h2d_async(d, v.data(), sizeof(T) * v.size(), s);
   return d;
 }
 
