@@ -53,6 +53,7 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 constexpr size_t kQrSmem = sizeof(double) * (2 * kChunk * kPanel + 2 * kPanel + kQT / 32);
+static_assert(kChunk == kQT, "one thread per row of a chunk");
 
 // Householder QR of one chunk (rows <= 256, w <= 32), LAPACK dlarfg
 // convention: H_j = I - tau_j v_j v_j^T, v_j(j) = 1, beta_j = -sign(x0)||x||.
@@ -99,11 +100,10 @@ __global__ void __launch_bounds__(kQT) qr_chunk_kernel(const QrChunk *__restrict
       if (lane == 0) wv[c] = dot * t;
     }
     __syncthreads();
-    const int nr = r - j, nc = w - j - 1;
-    for (int idx = tid; idx < nr * nc; idx += kQT) {
-      const int i = j + idx % nr, c = j + 1 + idx / nr;
-      const double vi = (i == j) ? 1.0 : S[i + j * kChunk];
-      S[i + c * kChunk] -= vi * wv[c];
+    // trailing update, one thread per row (no index division)
+    if (tid >= j && tid < r) {
+      const double vi = (tid == j) ? 1.0 : S[tid + j * kChunk];
+      for (int c = j + 1; c < w; ++c) S[tid + c * kChunk] -= vi * wv[c];
     }
     __syncthreads();
   }
@@ -128,11 +128,9 @@ __global__ void __launch_bounds__(kQT) qr_chunk_kernel(const QrChunk *__restrict
       if (lane == 0) wv[c] = dot * t;
     }
     __syncthreads();
-    const int nr = r - j, nc = w - j;
-    for (int idx = tid; idx < nr * nc; idx += kQT) {
-      const int i = j + idx % nr, c = j + idx / nr;
-      const double vi = (i == j) ? 1.0 : S[i + j * kChunk];
-      E[i + c * kChunk] -= vi * wv[c];
+    if (tid >= j && tid < r) {
+      const double vi = (tid == j) ? 1.0 : S[tid + j * kChunk];
+      for (int c = j; c < w; ++c) E[tid + c * kChunk] -= vi * wv[c];
     }
     __syncthreads();
   }
