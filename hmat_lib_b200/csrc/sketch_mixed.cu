@@ -46,9 +46,12 @@ SketchMixed::SketchMixed(const std::vector<SketchMixedBlock> &blocks, cudaStream
     cexp_off_[i] = nexp;
     nexp += B.n;
   }
-  HB_CUDA(cudaMalloc((void **)&slices_, std::max<long long>(bytes, 1)));
-  HB_CUDA(cudaMalloc((void **)&exps_, sizeof(int) * std::max<long long>(nexp, 1)));
-  HB_CUDA(cudaMalloc((void **)&status_, sizeof(int)));
+  // stream-ordered (the device's pool, kept mapped): a synchronous cudaMalloc
+  // of the slices (gigabytes) competed with the pool for physical memory
+  keep_pool_memory();
+  HB_CUDA(cudaMallocAsync((void **)&slices_, std::max<long long>(bytes, 1), s));
+  HB_CUDA(cudaMallocAsync((void **)&exps_, sizeof(int) * std::max<long long>(nexp, 1), s));
+  HB_CUDA(cudaMallocAsync((void **)&status_, sizeof(int), s));
   HB_CUDA(cudaMemsetAsync(status_, 0, sizeof(int), s));
   unsigned long long *maxabs = nullptr;
   HB_CUDA(cudaMallocAsync((void **)&maxabs, sizeof(unsigned long long) * std::max(nexp, 1LL), s));
@@ -82,9 +85,9 @@ SketchMixed::SketchMixed(const std::vector<SketchMixedBlock> &blocks, cudaStream
 }
 
 SketchMixed::~SketchMixed() {
-  cudaStreamSynchronize(stream_);
   for (void *p : {(void *)slices_, (void *)exps_, (void *)status_})
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, stream_);
+  cudaStreamSynchronize(stream_);
   for (void *p : keep_)
     if (p) cudaFree(p);
 }
