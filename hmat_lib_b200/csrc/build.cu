@@ -301,7 +301,6 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   struct ExactSlot { long long ws, u, v, sig; };
   std::vector<ExactSlot> eslots;
   int max_c = 0;
-  long long max_rc = 0;   // largest R C of an exact problem
   for (int b : exact) {
     const BlockDesc &B = blk[b].B;
     const int C = std::min(B.m, B.n);
@@ -312,7 +311,6 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     s.sig = take(C);
     eslots.push_back(s);
     max_c = std::max(max_c, C);
-    max_rc = std::max(max_rc, (long long)std::max(B.m, B.n) * C);
   }
   // Option build_precision = 1 (dense input only): the sketch products
   // Y = A Omega and B^T = A^T Q on the int8 tensor cores, every block sliced
@@ -557,10 +555,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   JacobiProb *d_eprobs = nullptr;
   if (!eprobs.empty()) {
     d_eprobs = upload_vec(eprobs, stream);
-    // blocks up to 128 x 128 keep their working copy in shared memory
-    JacobiParams pe = prm;
-    pe.smem_g = max_rc <= (long long)option("jacobi_smem_elems", 16384) ? max_rc : 0;
-    jacobi_svd_batched(d_eprobs, (int)eprobs.size(), pe, d_status, max_c, stream, gspec);
+    jacobi_svd_batched(d_eprobs, (int)eprobs.size(), prm, d_status, max_c, stream, gspec);
   }
 
   HB_CUDA(cudaEventRecord(ev[1], stream));
@@ -866,11 +861,7 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
     }
     if (!small.empty()) {
       d_sprobs = upload_vec(small, stream);
-      JacobiParams ps = prm;
-      ps.smem_g = (long long)max_l * max_l <= (long long)option("jacobi_smem_elems", 16384)
-                      ? (long long)max_l * max_l
-                      : 0;
-      jacobi_svd_batched(d_sprobs, (int)small.size(), ps, d_status, max_l, stream);
+      jacobi_svd_batched(d_sprobs, (int)small.size(), prm, d_status, max_l, stream);
     }
     if (!big.empty()) block_jacobi_svd(big, tol, prm.max_sweeps, d_status, stream);
   }

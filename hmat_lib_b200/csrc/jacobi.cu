@@ -101,12 +101,6 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
   __shared__ double s_team_off;
 
   double *G = P.G, *W = P.W;
-  // G in shared memory after s_sig and s_perm (16-byte aligned): every pair
-  // step then reads its columns at shared-memory latency instead of L1 / L2
-  if constexpr (!kTeam) {
-    if (prm.smem_g > 0 && (long long)R * C <= prm.smem_g)
-      G = sh + ((C + (C + 1) / 2 + 1) & ~1);
-  }
   const int gtid = crank * blockDim.x + tid, gthreads = team * blockDim.x;
   double fro2 = 0.0;   // this thread's share of ||A||_F^2
   for (long long e = gtid; e < (long long)R * C; e += gthreads) {
@@ -378,24 +372,16 @@ void jacobi_svd_batched(const JacobiProb *d_probs, int nprobs, const JacobiParam
   // problem a cluster of CTAs; the others one CTA
   const int team_min_c = (int)std::min(option("jacobi_cluster_min_c", 192.0), 1e9);
   if (max_c >= team_min_c) {
-    JacobiParams pc = prm;
-    pc.smem_g = 0;
     if (smem > 48 * 1024)
       HB_CUDA(cudaFuncSetAttribute(jacobi_svd_cluster_kernel,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     jacobi_svd_cluster_kernel<<<nprobs * kJCluster, kJThreads, smem, stream>>>(
-        d_probs, pc, d_status, team_min_c, gen);
+        d_probs, prm, d_status, team_min_c, gen);
   } else {
-    JacobiParams p1 = prm;
-    size_t smem1 = smem + 16;
-    if (p1.smem_g > 0 && smem1 + sizeof(double) * p1.smem_g <= 220 * 1024)
-      smem1 += sizeof(double) * p1.smem_g;
-    else
-      p1.smem_g = 0;
-    if (smem1 > 48 * 1024)
+    if (smem > 48 * 1024)
       HB_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem1));
-    jacobi_svd_kernel<<<nprobs, kJThreads, smem1, stream>>>(d_probs, p1, d_status, gen);
+                                   (int)smem));
+    jacobi_svd_kernel<<<nprobs, kJThreads, smem, stream>>>(d_probs, prm, d_status, gen);
   }
   HB_LAUNCHED();
 }

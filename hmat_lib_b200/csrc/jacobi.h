@@ -49,10 +49,6 @@ struct JacobiParams {
   // problems without their own conv_scale take ||A||_F: a pair also counts as
   // orthogonal when |g_p . g_q| <= conv_tol ||A||_F max(||g_p||, ||g_q||)
   int norm_stop = 0;
-  // one-CTA problems with R C <= smem_g (R = max(m, n), C = min(m, n)) keep
-  // G in shared memory instead of the workspace (the launch reserves smem_g
-  // doubles; 0: never; ignored by cluster launches)
-  long long smem_g = 0;
 };
 
 // Workspace doubles needed by problem (m, n): G + W.
