@@ -216,3 +216,21 @@ def test_sketch_growth_bounded_by_memory_budget(lib):
     lib.hodlr_b200_build_stats(st, 18)
     assert st[9] > 1024 and st[4] == 0   # largest sketch, cap hit
     t.free()
+
+
+@pytest.mark.parametrize("n,h", [(1024, 3), (4096, 5)])
+def test_highest_rank_and_workspace_on_built_trees(lib, n, h):
+    """get_highest_s is the largest off-diagonal rank of a built tree and
+    compute_multiply_hodlr_dense_workspace that rank times the column count
+    (hmat_lib src/utils.c:5-26, src/dense_algebra.c:39-44), on trees built by
+    dense_to_tree_hodlr."""
+    pts = W.points_1d_sorted(n, seed=5)
+    a = W.kernel_matrix(pts, "matern32", 0.2, 1e-2)
+    t = Tree.from_dense(a, h, 1e-10)
+    td = t.data()
+    highest = max(u.shape[1] for (u, v) in td.blocks.values())
+    assert highest > 1
+    assert lib.get_highest_s(t.tp) == highest
+    for k in (1, 7, 256):
+        assert lib.compute_multiply_hodlr_dense_workspace(t.tp, k) == highest * k
+    t.free()
