@@ -517,7 +517,6 @@ std::vector<std::shared_ptr<DeviceTree>> build_attempt(
   // off by default: the normalised columns of the rotated side (hmat_lib's
   // orthonormal U or V) then keep couplings of up to eps ||A|| / sigma
   prm.norm_stop = option("jacobi_norm_stop", 0.0) != 0.0 ? 1 : 0;
-  prm.pair_skip = option("jacobi_pair_skip", 0.01);
 
   // stage events: start, exact done, rounds done, core SVDs done, end
   cudaEvent_t ev[5];

@@ -149,16 +149,6 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
     theta = 1e-3 * prm.tol / sqrt((double)C);
   theta = fmax(theta, P.skip_abs);
   const double skip2 = theta * theta;
-  // Pairs of two columns both below pair_skip tol ||A||_F / sqrt(C) are
-  // neither rotated nor tested: all such columns together hold at most
-  // pair_skip tol ||A||_F <= pair_skip sqrt(C) tol s_0 (0.11 tol s_0 for
-  // pair_skip 0.01 and C = 128), so their unresolved couplings among
-  // themselves lift none of their singular values to the truncation
-  // threshold, and every pair with a larger column is still rotated (kept
-  // columns stay orthogonal to all others).
-  const double pskip2 = (prm.pair_skip > 0.0 && prm.trunc == Truncation::Relative)
-                            ? prm.pair_skip * prm.pair_skip * prm.tol * prm.tol * f2 / C
-                            : 0.0;
   const double cscale = P.conv_scale > 0.0 ? P.conv_scale : (prm.norm_stop ? sqrt(f2) : 0.0);
 
   // a computed dot product of length R carries ~sqrt(R) eps relative noise:
@@ -207,7 +197,6 @@ __device__ void jacobi_solve(const JacobiProb &P, const JacobiParams &prm, int *
         ga = warp_sum(ga);
         if (ga == 0.0 || al <= 0.0 || be <= 0.0) continue;
         if (al <= skip2 || be <= skip2) continue;
-        if (al <= pskip2 && be <= pskip2) continue;
         double rel = fabs(ga) / (sqrt(al) * sqrt(be));
         // coupling at rounding level of the problem's own scale (a block of a
         // larger matrix, whose columns were recomputed by a GEMM) counts as

@@ -49,9 +49,6 @@ struct JacobiParams {
   // problems without their own conv_scale take ||A||_F: a pair also counts as
   // orthogonal when |g_p . g_q| <= conv_tol ||A||_F max(||g_p||, ||g_q||)
   int norm_stop = 0;
-  // relative truncation: a pair whose two columns are both below
-  // pair_skip tol ||A||_F / sqrt(C) is neither rotated nor tested (0: off)
-  double pair_skip = 0.0;
 };
 
 // Workspace doubles needed by problem (m, n): G + W.

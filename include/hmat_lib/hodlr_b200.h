@@ -80,8 +80,6 @@ const char *hodlr_b200_last_error(void);
  *   exact_max (128): blocks with min(m, n) up to this are compressed by an
  *       exact Jacobi SVD
  *   jacobi_max_sweeps (60): Jacobi sweep bound (SVD_FAILURE past it)
- *   jacobi_pair_skip (0.01): in the build's Jacobi SVDs a pair of columns both
- *       below this times tol ||A||_F / sqrt(C) is not rotated (0: off)
  *   jacobi_norm_stop (0): 1 = in the build's one-CTA / cluster Jacobi SVDs a
  *       column pair also counts as orthogonal when its product is at rounding
  *       level of eps ||A||_F times the larger column norm (fewer sweeps; the
