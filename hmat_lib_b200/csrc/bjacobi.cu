@@ -45,7 +45,7 @@ constexpr int kBj = 32;          // columns per block
 constexpr int kPair = 2 * kBj;   // columns per pair
 constexpr int kLd = 68;          // leading dimension of the 64 x 64 tiles in shared memory
 constexpr int kPT = 256;         // threads of the pair kernel (8 warps)
-constexpr int kInner = 30;       // sweeps of a pair's eigensolver at most
+constexpr int kInner = 30;       // sweeps of a pair's eigensolver at most (option bj_inner_sweeps)
 constexpr int kT = 32;           // transpose tile
 constexpr int kMaxCluster = 8;
 
@@ -170,7 +170,8 @@ __device__ __forceinline__ void rotate_rows(double *xa, double *xb, long long ld
 
 // One round for every pair slot: blockIdx.x / cluster size = slot.
 __global__ void __launch_bounds__(kPT, 1)
-bj_pair_kernel(const BjDev *__restrict__ probs, const int2 *__restrict__ slots, long long g_round) {
+bj_pair_kernel(const BjDev *__restrict__ probs, const int2 *__restrict__ slots, long long g_round,
+               int inner_max) {
   extern __shared__ __align__(16) unsigned char bj_smem_raw[];
   PairSmem &S = *reinterpret_cast<PairSmem *>(bj_smem_raw);
   cg::cluster_group cl = cg::this_cluster();
@@ -274,7 +275,7 @@ bj_pair_kernel(const BjDev *__restrict__ probs, const int2 *__restrict__ slots, 
   __syncthreads();
   if (!S.work) return;   // the same decision in every CTA of the cluster
 
-  for (int sweep = 0; sweep < kInner; ++sweep) {
+  for (int sweep = 0; sweep < inner_max; ++sweep) {
     for (int step = 0; step < kPair - 1; ++step) {
       if (tid < kPair / 2) {
         int p, q;
@@ -470,6 +471,9 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
   BjDev *d_probs = upload_vec(hd, s);
   std::vector<int> rot(np, 0);
 
+  // A pair's eigensolver may stop before it converges: its rotation is still
+  // orthogonal, and the outer sweeps finish the job.
+  const int inner_max = std::max(1, std::min(kInner, (int)option("bj_inner_sweeps", kInner)));
   int dev = 0, nsm = 148;
   HB_CUDA(cudaGetDevice(&dev));
   HB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -516,7 +520,7 @@ void block_jacobi_svd(const std::vector<BjProb> &probs, double tol, int max_swee
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       HB_CUDA(cudaLaunchKernelEx(&cfg, bj_pair_kernel, (const BjDev *)d_probs,
-                                 (const int2 *)d_slots, g));
+                                 (const int2 *)d_slots, g, inner_max));
       HB_LAUNCHED();
     }
     // end of a sweep of some problem: a problem whose sweep rotated nothing

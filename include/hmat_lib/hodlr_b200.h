@@ -87,6 +87,8 @@ const char *hodlr_b200_last_error(void);
  *       about eps ||A|| / sigma)
  *   jacobi_cluster_min_c (192): problems this wide or wider use a cluster of
  *       8 CTAs
+ *   bj_inner_sweeps (30): sweeps of the block Jacobi SVD's per-pair eigensolver
+ *       at most (fewer: cheaper rounds, possibly more outer sweeps)
  *   jacobi_block_min_c (128): sketch cores this wide or wider are solved by
  *       the block Jacobi SVD (32-column blocks; per round one launch: Gram of
  *       each 64-column pair, its eigenvectors, in-place rotation)
